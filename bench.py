@@ -1,0 +1,375 @@
+#!/usr/bin/env python
+"""Headline benchmark: particle-steps/s of the Barnes-Hut step on the
+1,048,576-particle two-galaxy collision (theta = 0.5, eps = 0.02,
+dt = 0.0025, leaf <= 32, FP32 walk with FP64 centre-of-mass sums).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gcs|reference]
+
+One process per GPU (torchrun for N > 1, NCCL only for the barrier and the
+max-over-ranks time).  Every rank steps its own scenario (seed = rank): the
+path shards by scenario with no data-path collective, so scaling is weak.
+
+value   = N_particles * K * ranks / (max over ranks of the device time of K
+          steps), inputs resident in HBM (the 1M-particle working set,
+          ~270 MB, is larger than the 126 MB L2; no flush needed);
+e2e     = the same metric through the C ABI with host buffers: every step
+          copies the Star array in from pinned host memory and the stepped
+          Star array back out (gcs_upload_stars + gcs_step_host);
+roofline= the walk kernel (the dominant stage) against the FP32 FMA-pipe
+          peak: 20 flops per interaction (monopole or particle term),
+          interactions counted by the counting walk on the same state;
+cpu_baseline = the reference's own CPU Barnes-Hut (oracle/_ref/libref_cpu.so:
+          engine.cpp + gravity_aggregator.cpp at theta 0.5, OpenMP over all
+          host cores), timed on whole 1M-particle steps;
+ref_gpu = the reference's own GPU path (oracle/_ref/libref_cuda.so, theta
+          0.5, leaf 1, CUB sort) on the same scenario, device time of its
+          kernel sequence (cuda_engine.cu:394-424).
+--impl reference runs only the reference CPU implementation, as its own arm.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "galaxy-collision-simulator_b200"))
+
+import numpy as np  # noqa: E402
+
+N_DEFAULT = 1048576
+THETA, EPS, DT = 0.5, 0.02, 0.0025
+FLOPS_PER_INTERACTION = 20
+WORKLOAD = ("two-galaxy collision, 1,048,576 particles (2 x [384,000 MN disc + 96,000 Hernquist bulge + "
+            "44,288 Hernquist halo]), theta=0.5, eps=0.02, dt=0.0025, leaf<=32")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["gcs", "reference"], default="gcs")
+    ap.add_argument("--n", type=int, default=N_DEFAULT, help="particles (default: the 1M config)")
+    ap.add_argument("--leaf", type=int, default=0, help="leaf size (0: tuned default)")
+    ap.add_argument("--batch", type=int, default=0, help="walk nodes per pop (0: tuned default)")
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
+    return ap.parse_args()
+
+
+def counts_for(n):
+    """Per-galaxy disc/bulge/halo counts of the recipe, scaled to n."""
+    if n == N_DEFAULT:
+        return (384000, 96000, 44288)
+    if n == 45056:
+        return (16384, 4096, 2048)
+    g = n // 2
+    d = int(round(g * 384000 / 524288))
+    b = int(round(g * 96000 / 524288))
+    return (d, b, g - d - b)
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples (200 ms) while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def profile_traffic():
+    """dram bytes per walk launch from the committed ncu summary (or None)."""
+    path = os.path.join(ROOT, "profiles", "walk_1m.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":", 1)[1])
+    except (OSError, ValueError):
+        pass
+    return None
+
+
+def make_params(gcs, leaf, batch):
+    return gcs.reference_params(theta=THETA, epsilon_sq=EPS * EPS, dt=DT, leaf_size=leaf, walk_batch=batch,
+                                bounds_mode=gcs.BOUNDS_DEVICE, com_fp64=1, recolor=1)
+
+
+def cpu_reference_rate(stars, budget_s, max_steps=None):
+    """Time whole reference CPU steps on a copy of `stars` until the budget is spent."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle  # noqa: PLC0415
+    L = oracle.ref_lib("ref_cpu")
+    kind = "reference"
+    if L is None:
+        return None
+    n = len(stars)
+    st = np.ascontiguousarray(stars.copy())
+    L.ref_cpu_init(n, 1 << 28)
+    L.ref_cpu_set_theta(THETA)
+    steps, t_total = 0, 0.0
+    while True:
+        t0 = time.perf_counter()
+        rc = L.ref_cpu_step(st.ctypes.data, n, 1.0, EPS * EPS, DT, None, None)
+        t_total += time.perf_counter() - t0
+        if rc != 0:
+            raise RuntimeError("reference CPU step failed")
+        steps += 1
+        if t_total >= budget_s or (max_steps and steps >= max_steps):
+            break
+    L.ref_cpu_cleanup()
+    return {"value": n * steps / t_total, "unit": "particle-steps/s", "cores": int(L.ref_cpu_threads()),
+            "kind": kind, "steps": steps, "seconds": t_total,
+            "sample": "%d whole reference CPU steps (octree, leaf<=32, theta=0.5) of the %d-particle scenario"
+                      % (steps, n)}
+
+
+def ref_gpu_rate(stars, steps=3):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle  # noqa: PLC0415
+    if oracle.ref_lib("ref_cuda") is None:
+        return None
+    n = len(stars)
+    x = np.stack([stars["x"], stars["y"], stars["z"]])
+    lo, hi = float(x.min()), float(x.max())
+    pad = 0.05 * (hi - lo)
+    ref = oracle.RefCuda(n)
+    try:
+        ref.set_theta(THETA)
+        ref.upload(stars)
+        ref.step_device(1.0, EPS * EPS, DT, lo - pad, hi + pad)
+        ms = [ref.step_device(1.0, EPS * EPS, DT, lo - pad, hi + pad) for _ in range(steps)]
+        walk_ms = ref.time_walk(1.0, EPS * EPS)
+    finally:
+        ref.close()
+    t = statistics.median(ms)
+    return {"value": n / (t / 1e3), "unit": "particle-steps/s", "ms_per_step": t, "walk_ms": walk_ms,
+            "kind": "reference CUDA path (cuda_engine.cu:394-424, theta 0.5, leaf 1, CUB sort), sm_100a, "
+                    "device time, same GPU"}
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return 0
+    import gcs  # noqa: PLC0415
+    stars = gcs.collision_equal(*counts_for(args.n), seed=0)
+    n = len(stars)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle  # noqa: PLC0415
+    L = oracle.ref_lib("ref_cpu")
+    if L is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_cpu.so not built"}))
+        return 0
+    st = np.ascontiguousarray(stars.copy())
+    L.ref_cpu_init(n, 1 << 28)
+    L.ref_cpu_set_theta(THETA)
+    for _ in range(args.warmup):
+        L.ref_cpu_step(st.ctypes.data, n, 1.0, EPS * EPS, DT, None, None)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        L.ref_cpu_step(st.ctypes.data, n, 1.0, EPS * EPS, DT, None, None)
+    t = time.perf_counter() - t0
+    cores = int(L.ref_cpu_threads())
+    L.ref_cpu_cleanup()
+    value = n * args.steps / t
+    line = {"metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded two-galaxy initial conditions)", "impl": "reference",
+            "config": {"workload": WORKLOAD, "particles": n},
+            "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": cores, "kind": "reference",
+                             "sample": "%d whole steps of the reference CPU Barnes-Hut (engine.cpp, "
+                                       "gravity_aggregator.cpp, theta 0.5) after %d warm-up steps"
+                                       % (args.steps, args.warmup)},
+            "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference_arm(args, rank, world)
+
+    import torch  # noqa: PLC0415
+    import gcs  # noqa: PLC0415
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime  # noqa: PLC0415
+        import torch.distributed as dist  # noqa: PLC0415
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    stars = gcs.collision_equal(*counts_for(args.n), seed=rank)
+    n = len(stars)
+    leaf = args.leaf if args.leaf > 0 else 16
+    p = make_params(gcs, leaf, args.batch)
+    stream = torch.cuda.current_stream()
+    ctx = gcs.Context(n, device=local)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.upload(stars)
+    n_mono, n_part = ctx.count_interactions(p)
+    ctx.upload(stars)
+
+    for _ in range(args.warmup):
+        ctx.step(p)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    wev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    ev0.record(stream)
+    for k in range(args.steps):
+        ctx.run_stages(p, gcs.STAGE_BOUNDS, gcs.STAGE_AGGREGATE)
+        wev[k][0].record(stream)
+        ctx.run_stages(p, gcs.STAGE_WALK, gcs.STAGE_WALK)
+        wev[k][1].record(stream)
+        ctx.run_stages(p, gcs.STAGE_INTEGRATE, gcs.STAGE_INTEGRATE)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    status = ctx.device_status()
+    if status:
+        raise RuntimeError("device status word 0x%x after the timed steps" % status)
+    t_ms = ev0.elapsed_time(ev1)
+    walk_ms = sum(a.elapsed_time(b) for a, b in wev) / args.steps
+    t_max = t_ms
+    if dist is not None:
+        tt = torch.tensor([t_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+    value = n * args.steps * world / (t_max / 1e3)
+
+    # ---- end to end through the C ABI with host buffers
+    host = torch.empty(n * 32, dtype=torch.uint8, pin_memory=True)
+    hv = host.numpy().view(gcs.STAR_DTYPE)
+    ctx.download(out=hv)
+    ke = max(1, args.e2e_steps)
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(ke):
+        ctx.upload(hv)
+        ctx.step_host(p, hv)
+    t_e2e = time.perf_counter() - t0
+    if dist is not None:
+        tt = torch.tensor([t_e2e], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_e2e = float(tt.item())
+    e2e = {"value": n * ke * world / t_e2e, "unit": "particle-steps/s", "h2d_bytes_per_step": 32 * n,
+           "d2h_bytes_per_step": 32 * n, "steps": ke,
+           "path": "gcs_upload_stars (pinned Star[] H2D) + gcs_step_host (step, pack, Star[] D2H)"}
+
+    peaks = measured_peaks()
+    sm_max = float(peaks.get("sm_max_mhz", 1965.0))
+    props = torch.cuda.get_device_properties(local)
+    fp32_peak = props.multi_processor_count * 128 * 2 * sm_max * 1e6 / 1e12
+    inter = n_mono + n_part
+    achieved = inter * FLOPS_PER_INTERACTION / (walk_ms / 1e3) / 1e12
+    traffic = profile_traffic()
+    roofline = {"kernel": "walk_kernel", "bound": "fp32", "achieved": achieved, "peak": fp32_peak,
+                "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": traffic,
+                "peak_source": "derived: %d SMs x 128 FP32 lanes x 2 x sm_max_mhz %.0f (MEASURED_PEAKS.json); "
+                               "no FP32 figure is measured there" % (props.multi_processor_count, sm_max),
+                "walk_ms": walk_ms, "interactions_per_step": inter, "monopole_terms": n_mono,
+                "particle_terms": n_part, "interactions_per_s": inter / (walk_ms / 1e3)}
+    passes = 8
+    launches_per_step = 2 + 1 + passes + 1 + 1 + 1 + 1 + 1
+    line = {"metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded two-galaxy initial conditions, seed = rank)",
+            "config": {"workload": WORKLOAD, "particles": n, "leaf_size": leaf,
+                       "walk_batch": args.batch or 16, "com": "fp64 sums", "bounds": "device, per step",
+                       "l2": "working set ~270 MB > 126 MB L2; no flush", "parallelism": "replicas x%d" % world},
+            "e2e": e2e, "roofline": roofline, "clocks": clocks, "gpu_launches": launches_per_step * args.steps,
+            "device_status": status}
+    if rank == 0 and world == 1:
+        if not args.no_ref_gpu:
+            line["ref_gpu"] = ref_gpu_rate(stars)
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_reference_rate(stars, args.cpu_seconds)
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,625 @@
+// engine.cu - the gcs_ctx context behind include/gcs.h: device buffers,
+// segment layout, the per-step stage sequence and the C ABI.
+//
+// Replaces the reference's file-scope globals and cuda_physics_step
+// (cuda_engine.cu:16-44, 219-451).  Differences in structure, not in
+// results: state lives in a context (so several scenarios can share a
+// device), all work is asynchronous on the context's stream with no device
+// synchronisation between stages, and every failure is a status code.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "gcs_internal.h"
+
+using namespace gcs;
+
+struct gcs_ctx {
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+    int64_t capacity = 0;
+    int32_t max_segments = 1;
+
+    // layout
+    int32_t n = 0, nseg = 0, n_internal = 0;
+    std::vector<int64_t> h_seg_off;
+    int n_groups = 0, n_chunks = 0;
+
+    // device state
+    float4* pos[2] = {nullptr, nullptr};
+    float4* vel[2] = {nullptr, nullptr};
+    float4* acc = nullptr;
+    int cur = 0;
+    uint64_t* keys[2] = {nullptr, nullptr};
+    uint32_t* idx[2] = {nullptr, nullptr};
+    int sorted_buf = 0;
+    BvhNodeTraverse* tr = nullptr;
+    BvhNodeBuild* bd = nullptr;
+    double4* com64 = nullptr;
+    int32_t* leaf_parent = nullptr;
+    int64_t* seg_off = nullptr;
+    int32_t* seg_id = nullptr;
+    WalkGroup* groups = nullptr;
+    Chunk* chunks = nullptr;
+    float2* seg_bounds = nullptr;
+    Star* staging = nullptr;
+    PlaybackStar* pb_staging = nullptr;
+    unsigned char* scratch = nullptr;
+    size_t scratch_cap = 0;
+    uint32_t* status = nullptr;
+    double* diag = nullptr;
+    int64_t* targets = nullptr;
+    int64_t targets_cap = 0;
+    double* direct_out = nullptr;
+    unsigned long long* counts = nullptr;  // walk interaction counters (count mode)
+    bool count_walk = false;
+
+    std::string last_error;
+};
+
+namespace {
+
+constexpr int kChunkSize = 8192;
+// StepScratch rounded up to 256 bytes; the bounds and look-back regions follow.
+constexpr size_t kScratchHeader = (sizeof(StepScratch) + 255) & ~(size_t)255;
+static_assert(kScratchHeader >= sizeof(StepScratch), "scratch header must hold StepScratch");
+
+void set_error(gcs_ctx* c, const char* what, cudaError_t e) {
+    char buf[256];
+    snprintf(buf, sizeof buf, "%s: %s", what, cudaGetErrorString(e));
+    c->last_error = buf;
+}
+
+#define GCS_CUDA(ctx, call)                                  \
+    do {                                                     \
+        cudaError_t e_ = (call);                             \
+        if (e_ != cudaSuccess) {                             \
+            set_error((ctx), #call, e_);                     \
+            return GCS_ERR_CUDA;                             \
+        }                                                    \
+    } while (0)
+
+int check_launch(gcs_ctx* c, const char* stage) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error(c, stage, e);
+        return GCS_ERR_CUDA;
+    }
+    return GCS_OK;
+}
+
+Layout layout_of(const gcs_ctx* c) {
+    Layout L;
+    L.n = c->n;
+    L.nseg = c->nseg;
+    L.n_internal = c->n_internal;
+    L.seg_off = c->seg_off;
+    L.seg_id = c->seg_id;
+    return L;
+}
+
+int seg_passes(int nseg) { return nseg <= 1 ? 0 : (nseg <= 256 ? 1 : 2); }
+
+StepScratch* scratch_header(gcs_ctx* c) { return reinterpret_cast<StepScratch*>(c->scratch); }
+uint32_t* scratch_bounds(gcs_ctx* c) {
+    return reinterpret_cast<uint32_t*>(c->scratch + kScratchHeader);
+}
+uint32_t* scratch_lookback(gcs_ctx* c) {
+    size_t b = kScratchHeader + sizeof(uint32_t) * 2 * (size_t)c->max_segments;
+    b = (b + 255) & ~(size_t)255;
+    return reinterpret_cast<uint32_t*>(c->scratch + b);
+}
+size_t scratch_bytes_for(const gcs_ctx* c, int64_t n) {
+    size_t b = kScratchHeader + sizeof(uint32_t) * 2 * (size_t)c->max_segments;
+    b = (b + 255) & ~(size_t)255;
+    return b + sizeof(uint32_t) * sort_lookback_words(n, kKeyPasses + seg_passes(c->nseg));
+}
+
+template <typename T>
+int dalloc(gcs_ctx* c, T** p, size_t count) {
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), sizeof(T) * (count > 0 ? count : 1));
+    if (e != cudaSuccess) {
+        set_error(c, "cudaMalloc", e);
+        *p = nullptr;
+        return GCS_ERR_NOMEM;
+    }
+    return GCS_OK;
+}
+
+void free_all(gcs_ctx* c) {
+    void* ptrs[] = {c->pos[0], c->pos[1], c->vel[0], c->vel[1], c->acc, c->keys[0], c->keys[1],
+                    c->idx[0], c->idx[1], c->tr, c->bd, c->com64, c->leaf_parent, c->seg_off,
+                    c->seg_id, c->groups, c->chunks, c->seg_bounds, c->staging, c->pb_staging,
+                    c->scratch, c->status, c->diag, c->targets, c->direct_out, c->counts};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+}
+
+int validate_params(gcs_ctx* c, const gcs_params* p) {
+    if (!p) {
+        c->last_error = "null params";
+        return GCS_ERR_ARG;
+    }
+    if (p->leaf_size < 1 || p->leaf_size > 32) {
+        c->last_error = "leaf_size must be in [1, 32]";
+        return GCS_ERR_ARG;
+    }
+    if (p->bounds_mode != GCS_BOUNDS_CALLER && p->bounds_mode != GCS_BOUNDS_DEVICE) {
+        c->last_error = "bounds_mode must be GCS_BOUNDS_CALLER or GCS_BOUNDS_DEVICE";
+        return GCS_ERR_ARG;
+    }
+    if (!(p->theta >= 0.0f) || !(p->epsilon_sq >= 0.0f)) {
+        c->last_error = "theta and epsilon_sq must be >= 0";
+        return GCS_ERR_ARG;
+    }
+    return GCS_OK;
+}
+
+int default_walk_batch() { return 16; }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// stage sequence
+// ---------------------------------------------------------------------------
+static int run_stage(gcs_ctx* c, const gcs_params* p, int stage) {
+    cudaStream_t st = c->stream;
+    const Layout L = layout_of(c);
+    const int passes = kKeyPasses + seg_passes(c->nseg);
+    StepScratch* ss = scratch_header(c);
+    switch (stage) {
+        case GCS_STAGE_BOUNDS: {
+            GCS_CUDA(c, cudaMemsetAsync(c->scratch, 0, scratch_bytes_for(c, c->n), st));
+            if (p->bounds_mode == GCS_BOUNDS_DEVICE) {
+                launch_bounds(L, c->pos[c->cur], c->chunks, c->n_chunks, scratch_bounds(c),
+                              c->status, st);
+                launch_bounds_decode(scratch_bounds(c), c->seg_bounds, c->nseg, st);
+            }
+            return check_launch(c, "bounds");
+        }
+        case GCS_STAGE_ENCODE:
+            launch_encode(L, c->pos[c->cur], p->bounds_mode, p->global_min, p->global_max,
+                          c->seg_bounds, c->keys[0], c->idx[0], &ss->hist[0][0],
+                          seg_passes(c->nseg), st);
+            return check_launch(c, "encode");
+        case GCS_STAGE_SORT: {
+            for (int pass = 0; pass < passes; ++pass) {
+                const int in = pass & 1;
+                launch_sort_pass(L, pass, c->keys[in], c->idx[in], c->keys[in ^ 1], c->idx[in ^ 1],
+                                 &ss->hist[0][0], ss->tile_counter, scratch_lookback(c), c->status,
+                                 st);
+            }
+            c->sorted_buf = passes & 1;
+            return check_launch(c, "sort");
+        }
+        case GCS_STAGE_GATHER:
+            launch_gather(c->idx[c->sorted_buf], c->pos[c->cur], c->vel[c->cur], c->pos[c->cur ^ 1],
+                          c->vel[c->cur ^ 1], c->n, st);
+            c->cur ^= 1;
+            return check_launch(c, "gather");
+        case GCS_STAGE_BUILD:
+            launch_build(L, c->keys[c->sorted_buf], c->tr, c->bd, c->leaf_parent, c->status, st);
+            return check_launch(c, "build");
+        case GCS_STAGE_AGGREGATE:
+            launch_aggregate(L, c->pos[c->cur], c->tr, c->bd, c->com64, c->leaf_parent, p->com_fp64,
+                             c->status, st);
+            return check_launch(c, "aggregate");
+        case GCS_STAGE_WALK: {
+            WalkParams wp;
+            wp.G = p->G;
+            wp.eps2 = p->epsilon_sq;
+            wp.theta2 = p->theta * p->theta;
+            wp.leaf_size = p->leaf_size;
+            wp.batch = p->walk_batch > 0 ? p->walk_batch : default_walk_batch();
+            wp.with_potential = p->with_potential ? 1 : 0;
+            launch_walk(L, wp, c->pos[c->cur], c->tr, c->groups, c->n_groups, c->acc,
+                        &ss->walk_counter, c->status, p->walk_blocks_per_sm, c->sm_count,
+                        c->count_walk ? c->counts : nullptr, st);
+            return check_launch(c, "walk");
+        }
+        case GCS_STAGE_INTEGRATE:
+            launch_integrate(c->pos[c->cur], c->vel[c->cur], c->acc, p->dt, p->recolor, c->n, st);
+            return check_launch(c, "integrate");
+        default:
+            c->last_error = "unknown stage";
+            return GCS_ERR_ARG;
+    }
+}
+
+static int run_stages(gcs_ctx* c, const gcs_params* p, int first, int last) {
+    if (!c) return GCS_ERR_ARG;
+    int rc = validate_params(c, p);
+    if (rc) return rc;
+    if (first < GCS_STAGE_BOUNDS || last > GCS_STAGE_INTEGRATE || first > last) {
+        c->last_error = "bad stage range";
+        return GCS_ERR_ARG;
+    }
+    if (c->n <= 0) {
+        c->last_error = "no particles";
+        return GCS_ERR_STATE;
+    }
+    for (int s = first; s <= last; ++s) {
+        rc = run_stage(c, p, s);
+        if (rc) return rc;
+    }
+    return GCS_OK;
+}
+
+int gcs::pack_to_device(gcs_ctx* c, Star* dst) {
+    if (!c || !dst) return GCS_ERR_ARG;
+    cudaSetDevice(c->device);
+    launch_pack_stars(c->pos[c->cur], c->vel[c->cur], dst, c->n, c->stream);
+    int rc = check_launch(c, "pack_to_device");
+    if (rc) return rc;
+    GCS_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GCS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+void gcs_params_reference(gcs_params* p) {
+    if (!p) return;
+    memset(p, 0, sizeof *p);
+    p->G = 1.0f;
+    p->epsilon_sq = 10.0f;
+    p->theta = 1.0f;
+    p->dt = 0.01f;
+    p->leaf_size = 1;
+    p->bounds_mode = GCS_BOUNDS_CALLER;
+    p->global_min = -10000.0f;
+    p->global_max = 10000.0f;
+    p->recolor = 1;
+    p->com_fp64 = 0;
+    p->walk_batch = 0;
+    p->walk_blocks_per_sm = 0;
+}
+
+const char* gcs_status_string(int status) {
+    switch (status) {
+        case GCS_OK: return "ok";
+        case GCS_ERR_ARG: return "invalid argument";
+        case GCS_ERR_CUDA: return "CUDA runtime error";
+        case GCS_ERR_NOMEM: return "out of memory";
+        case GCS_ERR_CAPACITY: return "capacity exceeded";
+        case GCS_ERR_DEVICE: return "device status word set";
+        case GCS_ERR_STATE: return "invalid state";
+        case GCS_ERR_NO_DEVICE: return "no usable CUDA device";
+        default: return "unknown status";
+    }
+}
+
+const char* gcs_last_error(const gcs_ctx* c) { return c ? c->last_error.c_str() : "null context"; }
+
+int gcs_create(gcs_ctx** out, int64_t capacity, int32_t max_segments, int32_t device) {
+    if (!out || capacity < 1 || capacity > (int64_t)(1 << 30) - 1 || max_segments < 1 ||
+        max_segments > 65536)
+        return GCS_ERR_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device || device < 0) {
+        cudaGetLastError();
+        return GCS_ERR_NO_DEVICE;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return GCS_ERR_NO_DEVICE;
+    if (prop.major != 10) return GCS_ERR_NO_DEVICE;  // built for sm_100a only
+    if (cudaSetDevice(device) != cudaSuccess) return GCS_ERR_NO_DEVICE;
+
+    gcs_ctx* c = new gcs_ctx();
+    c->device = device;
+    c->sm_count = prop.multiProcessorCount;
+    c->capacity = capacity;
+    c->max_segments = max_segments;
+    const size_t N = (size_t)capacity;
+    const size_t max_groups = N / kGroupSize + (size_t)max_segments + 1;
+    const size_t max_chunks = N / kChunkSize + (size_t)max_segments + 1;
+    int rc = GCS_OK;
+    for (int b = 0; b < 2 && !rc; ++b) {
+        rc |= dalloc(c, &c->pos[b], N);
+        rc |= dalloc(c, &c->vel[b], N);
+        rc |= dalloc(c, &c->keys[b], N);
+        rc |= dalloc(c, &c->idx[b], N);
+    }
+    if (!rc) rc |= dalloc(c, &c->acc, N);
+    if (!rc) rc |= dalloc(c, &c->tr, N);
+    if (!rc) rc |= dalloc(c, &c->bd, N);
+    if (!rc) rc |= dalloc(c, &c->com64, N);
+    if (!rc) rc |= dalloc(c, &c->leaf_parent, N);
+    if (!rc) rc |= dalloc(c, &c->seg_off, (size_t)max_segments + 1);
+    if (!rc) rc |= dalloc(c, &c->seg_id, N);
+    if (!rc) rc |= dalloc(c, &c->groups, max_groups);
+    if (!rc) rc |= dalloc(c, &c->chunks, max_chunks);
+    if (!rc) rc |= dalloc(c, &c->seg_bounds, (size_t)max_segments);
+    if (!rc) rc |= dalloc(c, &c->staging, N);
+    if (!rc) rc |= dalloc(c, &c->pb_staging, N);
+    if (!rc) rc |= dalloc(c, &c->status, 1);
+    if (!rc) rc |= dalloc(c, &c->diag, 8);
+    if (!rc) rc |= dalloc(c, &c->counts, 2);
+    if (!rc) {
+        c->nseg = max_segments;  // worst case for the scratch size
+        c->scratch_cap = scratch_bytes_for(c, capacity) + 256;
+        c->nseg = 0;
+        rc |= dalloc(c, &c->scratch, c->scratch_cap);
+    }
+    if (rc) {
+        free_all(c);
+        delete c;
+        return GCS_ERR_NOMEM;
+    }
+    cudaMemset(c->status, 0, sizeof(uint32_t));
+    cudaMemset(c->acc, 0, sizeof(float4) * N);
+    int64_t cnt = capacity;
+    rc = gcs_set_segments(c, 1, &cnt);
+    if (rc) {
+        free_all(c);
+        delete c;
+        return rc;
+    }
+    *out = c;
+    return GCS_OK;
+}
+
+void gcs_destroy(gcs_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    else cudaDeviceSynchronize();
+    free_all(c);
+    delete c;
+}
+
+int gcs_set_stream(gcs_ctx* c, void* stream) {
+    if (!c) return GCS_ERR_ARG;
+    c->stream = reinterpret_cast<cudaStream_t>(stream);
+    return GCS_OK;
+}
+
+void* gcs_get_stream(const gcs_ctx* c) { return c ? reinterpret_cast<void*>(c->stream) : nullptr; }
+
+int gcs_set_segments(gcs_ctx* c, int32_t num_segments, const int64_t* counts) {
+    if (!c || num_segments < 1 || !counts) return GCS_ERR_ARG;
+    if (num_segments > c->max_segments) {
+        c->last_error = "more segments than max_segments";
+        return GCS_ERR_CAPACITY;
+    }
+    std::vector<int64_t> off((size_t)num_segments + 1, 0);
+    for (int s = 0; s < num_segments; ++s) {
+        if (counts[s] < 1) {
+            c->last_error = "every segment needs at least one particle";
+            return GCS_ERR_ARG;
+        }
+        off[s + 1] = off[s] + counts[s];
+    }
+    if (off[num_segments] > c->capacity) {
+        c->last_error = "segments exceed the context capacity";
+        return GCS_ERR_CAPACITY;
+    }
+    const int64_t n = off[num_segments];
+    std::vector<int32_t> sid((size_t)n);
+    std::vector<WalkGroup> groups;
+    std::vector<Chunk> chunks;
+    groups.reserve((size_t)(n / kGroupSize + num_segments));
+    for (int s = 0; s < num_segments; ++s) {
+        for (int64_t i = off[s]; i < off[s + 1]; ++i) sid[(size_t)i] = s;
+        for (int64_t g = off[s]; g < off[s + 1]; g += kGroupSize) {
+            WalkGroup w;
+            w.start = (int32_t)g;
+            w.count = (int32_t)std::min<int64_t>(kGroupSize, off[s + 1] - g);
+            w.seg = s;
+            w.pad = 0;
+            groups.push_back(w);
+        }
+        for (int64_t g = off[s]; g < off[s + 1]; g += kChunkSize) {
+            Chunk ch;
+            ch.start = (int32_t)g;
+            ch.count = (int32_t)std::min<int64_t>(kChunkSize, off[s + 1] - g);
+            ch.seg = s;
+            ch.pad = 0;
+            chunks.push_back(ch);
+        }
+    }
+    cudaSetDevice(c->device);
+    GCS_CUDA(c, cudaMemcpy(c->seg_off, off.data(), sizeof(int64_t) * off.size(), cudaMemcpyHostToDevice));
+    GCS_CUDA(c, cudaMemcpy(c->seg_id, sid.data(), sizeof(int32_t) * sid.size(), cudaMemcpyHostToDevice));
+    GCS_CUDA(c, cudaMemcpy(c->groups, groups.data(), sizeof(WalkGroup) * groups.size(),
+                           cudaMemcpyHostToDevice));
+    GCS_CUDA(c, cudaMemcpy(c->chunks, chunks.data(), sizeof(Chunk) * chunks.size(),
+                           cudaMemcpyHostToDevice));
+    c->h_seg_off = off;
+    c->n = (int32_t)n;
+    c->nseg = num_segments;
+    c->n_internal = (int32_t)(n - num_segments);
+    c->n_groups = (int)groups.size();
+    c->n_chunks = (int)chunks.size();
+    c->cur = 0;
+    return GCS_OK;
+}
+
+int64_t gcs_num_particles(const gcs_ctx* c) { return c ? c->n : 0; }
+int32_t gcs_num_segments(const gcs_ctx* c) { return c ? c->nseg : 0; }
+int64_t gcs_num_internal_nodes(const gcs_ctx* c) { return c ? c->n_internal : 0; }
+
+int gcs_upload_stars(gcs_ctx* c, const Star* host, int64_t offset, int64_t n) {
+    if (!c || !host || offset < 0 || n < 0 || offset + n > c->n) return GCS_ERR_ARG;
+    if (n == 0) return GCS_OK;
+    cudaSetDevice(c->device);
+    GCS_CUDA(c, cudaMemcpyAsync(c->staging + offset, host, sizeof(Star) * (size_t)n,
+                                cudaMemcpyHostToDevice, c->stream));
+    launch_unpack_stars(c->staging + offset, c->pos[c->cur] + offset, c->vel[c->cur] + offset, n,
+                        c->stream);
+    int rc = check_launch(c, "unpack");
+    if (rc) return rc;
+    GCS_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GCS_OK;
+}
+
+int gcs_download_stars(gcs_ctx* c, Star* host, int64_t offset, int64_t n) {
+    if (!c || !host || offset < 0 || n < 0 || offset + n > c->n) return GCS_ERR_ARG;
+    if (n == 0) return GCS_OK;
+    cudaSetDevice(c->device);
+    launch_pack_stars(c->pos[c->cur] + offset, c->vel[c->cur] + offset, c->staging + offset, n,
+                      c->stream);
+    int rc = check_launch(c, "pack");
+    if (rc) return rc;
+    GCS_CUDA(c, cudaMemcpyAsync(host, c->staging + offset, sizeof(Star) * (size_t)n,
+                                cudaMemcpyDeviceToHost, c->stream));
+    GCS_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GCS_OK;
+}
+
+int gcs_download_playback(gcs_ctx* c, PlaybackStar* host, int64_t offset, int64_t n) {
+    if (!c || !host || offset < 0 || n < 0 || offset + n > c->n) return GCS_ERR_ARG;
+    if (n == 0) return GCS_OK;
+    cudaSetDevice(c->device);
+    launch_pack_playback(c->pos[c->cur] + offset, c->vel[c->cur] + offset, c->pb_staging + offset,
+                         n, c->stream);
+    int rc = check_launch(c, "pack_playback");
+    if (rc) return rc;
+    GCS_CUDA(c, cudaMemcpyAsync(host, c->pb_staging + offset, sizeof(PlaybackStar) * (size_t)n,
+                                cudaMemcpyDeviceToHost, c->stream));
+    GCS_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GCS_OK;
+}
+
+int gcs_step(gcs_ctx* c, const gcs_params* p) {
+    if (!c) return GCS_ERR_ARG;
+    return run_stages(c, p, GCS_STAGE_BOUNDS, GCS_STAGE_INTEGRATE);
+}
+
+int gcs_step_host(gcs_ctx* c, const gcs_params* p, Star* host) {
+    if (!c || !host) return GCS_ERR_ARG;
+    int rc = run_stages(c, p, GCS_STAGE_BOUNDS, GCS_STAGE_INTEGRATE);
+    if (rc) return rc;
+    return gcs_download_stars(c, host, 0, c->n);
+}
+
+int gcs_compute_accels(gcs_ctx* c, const gcs_params* p) {
+    if (!c) return GCS_ERR_ARG;
+    return run_stages(c, p, GCS_STAGE_BOUNDS, GCS_STAGE_WALK);
+}
+
+int gcs_kick(gcs_ctx* c, float dt) {
+    if (!c) return GCS_ERR_ARG;
+    launch_kick(c->vel[c->cur], c->acc, dt, c->n, c->stream);
+    return check_launch(c, "kick");
+}
+
+int gcs_run_stages(gcs_ctx* c, const gcs_params* p, int32_t first, int32_t last) {
+    return run_stages(c, p, first, last);
+}
+
+int gcs_device_status(gcs_ctx* c, uint32_t* status, int32_t clear) {
+    if (!c || !status) return GCS_ERR_ARG;
+    cudaSetDevice(c->device);
+    GCS_CUDA(c, cudaStreamSynchronize(c->stream));
+    GCS_CUDA(c, cudaMemcpy(status, c->status, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (clear) GCS_CUDA(c, cudaMemset(c->status, 0, sizeof(uint32_t)));
+    return GCS_OK;
+}
+
+int gcs_synchronize(gcs_ctx* c) {
+    uint32_t s = 0;
+    int rc = gcs_device_status(c, &s, 0);
+    if (rc) return rc;
+    if (s) {
+        char buf[96];
+        snprintf(buf, sizeof buf, "device status word 0x%x", s);
+        c->last_error = buf;
+        return GCS_ERR_DEVICE;
+    }
+    return GCS_OK;
+}
+
+int gcs_read_buffer(gcs_ctx* c, int32_t which, void* host, int64_t first, int64_t count) {
+    if (!c || !host || first < 0 || count < 0) return GCS_ERR_ARG;
+    const void* src = nullptr;
+    size_t elem = 0;
+    int64_t limit = 0;
+    switch (which) {
+        case GCS_BUF_KEYS: src = c->keys[c->sorted_buf]; elem = 8; limit = c->n; break;
+        case GCS_BUF_INDEX: src = c->idx[c->sorted_buf]; elem = 4; limit = c->n; break;
+        case GCS_BUF_NODES: src = c->tr; elem = sizeof(BvhNodeTraverse); limit = c->n_internal; break;
+        case GCS_BUF_BUILD: src = c->bd; elem = sizeof(BvhNodeBuild); limit = c->n_internal; break;
+        case GCS_BUF_LEAF_PARENT: src = c->leaf_parent; elem = 4; limit = c->n; break;
+        case GCS_BUF_ACCEL: src = c->acc; elem = 16; limit = c->n; break;
+        case GCS_BUF_POS: src = c->pos[c->cur]; elem = 16; limit = c->n; break;
+        case GCS_BUF_VEL: src = c->vel[c->cur]; elem = 16; limit = c->n; break;
+        case GCS_BUF_BOUNDS: src = c->seg_bounds; elem = 8; limit = c->nseg; break;
+        case GCS_BUF_KEYS_UNSORTED: src = c->keys[0]; elem = 8; limit = c->n; break;
+        default: return GCS_ERR_ARG;
+    }
+    if (first + count > limit) return GCS_ERR_ARG;
+    if (count == 0) return GCS_OK;
+    cudaSetDevice(c->device);
+    GCS_CUDA(c, cudaStreamSynchronize(c->stream));
+    GCS_CUDA(c, cudaMemcpy(host, static_cast<const char*>(src) + elem * (size_t)first,
+                           elem * (size_t)count, cudaMemcpyDeviceToHost));
+    return GCS_OK;
+}
+
+int gcs_diagnostics(gcs_ctx* c, int32_t segment, double out[6]) {
+    if (!c || !out || segment < 0 || segment >= c->nseg) return GCS_ERR_ARG;
+    cudaSetDevice(c->device);
+    const int64_t first = c->h_seg_off[segment];
+    const int64_t n = c->h_seg_off[segment + 1] - first;
+    GCS_CUDA(c, cudaMemsetAsync(c->diag, 0, sizeof(double) * 6, c->stream));
+    launch_diag(c->pos[c->cur], c->vel[c->cur], c->acc, first, n, c->diag, c->stream);
+    int rc = check_launch(c, "diag");
+    if (rc) return rc;
+    GCS_CUDA(c, cudaMemcpyAsync(out, c->diag, sizeof(double) * 6, cudaMemcpyDeviceToHost, c->stream));
+    GCS_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GCS_OK;
+}
+
+int gcs_count_interactions(gcs_ctx* c, const gcs_params* p, uint64_t out[2]) {
+    if (!c || !p || !out) return GCS_ERR_ARG;
+    cudaSetDevice(c->device);
+    GCS_CUDA(c, cudaMemsetAsync(c->counts, 0, 2 * sizeof(unsigned long long), c->stream));
+    c->count_walk = true;
+    const int rc = run_stages(c, p, GCS_STAGE_BOUNDS, GCS_STAGE_WALK);
+    c->count_walk = false;
+    if (rc) return rc;
+    GCS_CUDA(c, cudaMemcpyAsync(out, c->counts, 2 * sizeof(uint64_t), cudaMemcpyDeviceToHost, c->stream));
+    GCS_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GCS_OK;
+}
+
+int gcs_direct_accels_fp64(gcs_ctx* c, const gcs_params* p, int32_t segment,
+                           const int64_t* targets, int64_t n_targets, double* out) {
+    if (!c || !p || !targets || !out || segment < 0 || segment >= c->nseg || n_targets < 0)
+        return GCS_ERR_ARG;
+    if (n_targets == 0) return GCS_OK;
+    const int64_t first = c->h_seg_off[segment];
+    const int64_t n = c->h_seg_off[segment + 1] - first;
+    for (int64_t i = 0; i < n_targets; ++i)
+        if (targets[i] < 0 || targets[i] >= n) return GCS_ERR_ARG;
+    cudaSetDevice(c->device);
+    if (n_targets > c->targets_cap) {
+        if (c->targets) cudaFree(c->targets);
+        if (c->direct_out) cudaFree(c->direct_out);
+        c->targets = nullptr;
+        c->direct_out = nullptr;
+        c->targets_cap = 0;
+        if (dalloc(c, &c->targets, (size_t)n_targets) || dalloc(c, &c->direct_out, 3 * (size_t)n_targets))
+            return GCS_ERR_NOMEM;
+        c->targets_cap = n_targets;
+    }
+    GCS_CUDA(c, cudaMemcpyAsync(c->targets, targets, sizeof(int64_t) * (size_t)n_targets,
+                                cudaMemcpyHostToDevice, c->stream));
+    launch_direct_fp64(c->pos[c->cur], first, n, c->targets, n_targets, (double)p->G,
+                       (double)p->epsilon_sq, c->direct_out, c->stream);
+    int rc = check_launch(c, "direct_fp64");
+    if (rc) return rc;
+    GCS_CUDA(c, cudaMemcpyAsync(out, c->direct_out, sizeof(double) * 3 * (size_t)n_targets,
+                                cudaMemcpyDeviceToHost, c->stream));
+    GCS_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GCS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,119 @@
+// gcs_internal.h - declarations shared by the engine's translation units.
+//
+// Device arrays (one context, N particles in S segments, n_internal = N - S):
+//   pos[2]   float4 x,y,z,mass           (ping-pong across the gather)
+//   vel[2]   float4 vx,vy,vz,bits(tcol)  (tcol = type | r<<8 | g<<16 | b<<24,
+//                                         the byte order of Star bytes 28..31)
+//   acc      float4 ax,ay,az,potential
+//   keys[2]  u64 Morton codes, idx[2] u32 positions (radix-sort ping-pong)
+//   nodes_tr BvhNodeTraverse[n_internal], nodes_bd BvhNodeBuild[n_internal]
+//   com64    double4 [n_internal] FP64 mass-weighted position sums
+//   leaf_parent i32[N]
+//   seg_off  i64[S+1], seg_id i32[N], groups int4[n_groups]
+//   scratch  zeroed once per step (sort histograms, tile counters, look-back,
+//            walk work counter, device bounds)
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "../../include/gcs_types.h"
+#include "../../include/gcs.h"
+
+namespace gcs {
+
+constexpr int kRadixBits = 8;
+constexpr int kRadix = 1 << kRadixBits;
+constexpr int kKeyPasses = 8;          // 63 Morton bits in 8-bit digits
+constexpr int kMaxPasses = 10;         // + up to two segment-id digits
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys per tile
+constexpr int kGroupSize = 32;         // walk targets per warp group
+
+// Work unit of the walk: up to 32 consecutive sorted particles of one segment.
+struct WalkGroup {
+    int32_t start;
+    int32_t count;
+    int32_t seg;
+    int32_t pad;
+};
+
+// Per-segment bounds chunk: a range of particles of one segment.
+struct Chunk {
+    int32_t start;
+    int32_t count;
+    int32_t seg;
+    int32_t pad;
+};
+
+// Layout of the concatenated segments as the kernels see it.
+struct Layout {
+    int32_t n;            // particles
+    int32_t nseg;         // segments
+    int32_t n_internal;   // n - nseg
+    const int64_t* seg_off;  // device [nseg+1]
+    const int32_t* seg_id;   // device [n]
+};
+
+// Scratch zeroed at the start of each step (one memset).
+struct StepScratch {
+    uint32_t hist[kMaxPasses][kRadix];    // global digit histograms
+    uint32_t tile_counter[kMaxPasses];    // onesweep tile ticket per pass
+    uint32_t walk_counter;                // walk work-queue head
+    uint32_t pad[5];
+    // followed by: bounds u32[2*S] (ordered-float max of -min / max),
+    //              look-back u32[passes][tiles][256]
+};
+
+// ---- launchers (one per stage; all asynchronous on `st`) ----------------
+void launch_unpack_stars(const Star* stars, float4* pos, float4* vel, int64_t n, cudaStream_t st);
+void launch_pack_stars(const float4* pos, const float4* vel, Star* out, int64_t n, cudaStream_t st);
+void launch_pack_playback(const float4* pos, const float4* vel, PlaybackStar* out, int64_t n,
+                          cudaStream_t st);
+
+void launch_bounds(const Layout& L, const float4* pos, const Chunk* chunks, int n_chunks,
+                   uint32_t* bounds_enc, uint32_t* status, cudaStream_t st);
+void launch_bounds_decode(const uint32_t* bounds_enc, float2* bounds, int nseg, cudaStream_t st);
+void launch_encode(const Layout& L, const float4* pos, int bounds_mode, float gmin, float gmax,
+                   const float2* seg_bounds, uint64_t* keys, uint32_t* idx, uint32_t* hist,
+                   int n_seg_passes, cudaStream_t st);
+
+size_t sort_lookback_words(int64_t n, int passes);
+void launch_sort_pass(const Layout& L, int pass, const uint64_t* keys_in, const uint32_t* vals_in,
+                      uint64_t* keys_out, uint32_t* vals_out, const uint32_t* hist,
+                      uint32_t* tile_counter, uint32_t* lookback, uint32_t* status,
+                      cudaStream_t st);
+
+void launch_gather(const uint32_t* idx, const float4* pos_in, const float4* vel_in, float4* pos_out,
+                   float4* vel_out, int64_t n, cudaStream_t st);
+void launch_build(const Layout& L, const uint64_t* keys, BvhNodeTraverse* tr, BvhNodeBuild* bd,
+                  int32_t* leaf_parent, uint32_t* status, cudaStream_t st);
+void launch_aggregate(const Layout& L, const float4* pos, BvhNodeTraverse* tr, BvhNodeBuild* bd,
+                      double4* com64, const int32_t* leaf_parent, int com_fp64, uint32_t* status,
+                      cudaStream_t st);
+
+struct WalkParams {
+    float G, eps2, theta2;
+    int32_t leaf_size;
+    int32_t batch;
+    int32_t with_potential;
+};
+void launch_walk(const Layout& L, const WalkParams& wp, const float4* pos,
+                 const BvhNodeTraverse* tr, const WalkGroup* groups, int n_groups,
+                 float4* acc, uint32_t* work_counter, uint32_t* status, int blocks_per_sm,
+                 int sm_count, unsigned long long* counts, cudaStream_t st);
+int walk_max_blocks_per_sm(int batch, int with_potential);
+
+void launch_integrate(float4* pos, float4* vel, const float4* acc, float dt, int recolor,
+                      int64_t n, cudaStream_t st);
+void launch_kick(float4* vel, const float4* acc, float dt, int64_t n, cudaStream_t st);
+
+void launch_diag(const float4* pos, const float4* vel, const float4* acc, int64_t first, int64_t n,
+                 double* out6, cudaStream_t st);
+// Pack the context's current particles as Star[] into a device buffer and
+// wait for it (the headless interop target of the drop-in API).
+int pack_to_device(gcs_ctx* c, Star* dst);
+
+void launch_direct_fp64(const float4* pos, int64_t seg_first, int64_t seg_n, const int64_t* targets,
+                        int64_t n_targets, double G, double eps2, double* out, cudaStream_t st);
+
+}  // namespace gcs

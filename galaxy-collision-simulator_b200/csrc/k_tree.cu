@@ -1,0 +1,207 @@
+// k_tree.cu - Karras (2012) binary radix tree over each segment's sorted
+// Morton keys, and the bottom-up aggregation of bounds, mass and centre of
+// mass.
+//
+// Build: one thread per internal node, as in karras_bvh.cuh:73-131.  The
+// steps of the published algorithm (direction from the neighbours' common
+// prefixes, exponential then binary search for the far end, binary search
+// for the split) decide the topology, so they are the same steps; the
+// common-prefix function is the reference's, including its duplicate-key
+// rule (equal keys compare their positions, karras_bvh.cuh:23-31).  Indices
+// are local to the segment, so a segment's tree is the tree the reference
+// builds for that segment alone.  Each node also records the far end of its
+// particle range, which gives the walk the node's particle count.
+//
+// Aggregation: one thread per particle climbs from its leaf; at each node the
+// first arrival stops and the second computes the node from both children
+// (karras_bvh.cuh:175-225).  Unlike the reference, the arrival counter is a
+// release/acquire handshake (__threadfence on both sides and L2-coherent
+// loads of the children), so the second arrival always sees the first one's
+// writes.  Centres of mass are either the reference's FP32 formula or FP64
+// mass-weighted sums carried up the tree (exact for leaf terms, no
+// cancellation at the top of the tree), rounded once to FP32.
+#include "gcs_internal.h"
+#include "device_math.cuh"
+
+namespace gcs {
+
+namespace {
+
+// Common prefix length of sorted keys i and j of one segment (local indices);
+// -1 when j falls outside the segment.
+__device__ __forceinline__ int lcp(int i, int j, int n, const uint64_t* __restrict__ k,
+                                   uint64_t ki) {
+    if (j < 0 || j >= n) return -1;
+    const uint64_t kj = __ldg(k + j);
+    if (ki == kj) return 64 + __clz(i ^ j);
+    return __clzll(ki ^ kj);
+}
+
+__global__ void build_kernel(Layout L, const uint64_t* __restrict__ keys,
+                             BvhNodeTraverse* __restrict__ tr, BvhNodeBuild* __restrict__ bd,
+                             int32_t* __restrict__ leaf_parent, uint32_t* __restrict__ status) {
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < L.n; g += gridDim.x * blockDim.x) {
+        const int s = L.nseg > 1 ? __ldg(L.seg_id + g) : 0;
+        const int off = (int)__ldg(L.seg_off + s);
+        const int n = (int)__ldg(L.seg_off + s + 1) - off;
+        const int i = g - off;                  // local index
+        const int node_base = off - s;          // first internal node of the segment
+        const int leaf_base = L.n_internal + off;
+        const uint64_t* k = keys + off;
+        if (n == 1) {                           // single particle: its leaf is the root
+            leaf_parent[g] = -1;
+            continue;
+        }
+        if (i >= n - 1) continue;
+        const uint64_t ki = __ldg(k + i);
+        const int d = (lcp(i, i + 1, n, k, ki) - lcp(i, i - 1, n, k, ki)) > 0 ? 1 : -1;
+        const int dmin = lcp(i, i - d, n, k, ki);
+        int lmax = 2;
+        while (lcp(i, i + lmax * d, n, k, ki) > dmin) lmax *= 2;
+        int l = 0;
+        for (int t = lmax / 2; t >= 1; t /= 2)
+            if (lcp(i, i + (l + t) * d, n, k, ki) > dmin) l += t;
+        const int j = i + l * d;
+        const int dnode = lcp(i, j, n, k, ki);
+        int s_ = 0, step = l;
+        do {
+            step = (step + 1) >> 1;
+            if (lcp(i, i + (s_ + step) * d, n, k, ki) > dnode) s_ += step;
+        } while (step > 1);
+        const int split = i + s_ * d + (d > 0 ? 0 : -1);
+        const int lo = min(i, j), hi = max(i, j);
+        if (split < lo || split + 1 > hi) atomicOr(status, GCS_DEV_BUILD_RANGE);
+        const int node = node_base + i;
+        const int cl = (lo == split) ? leaf_base + split : node_base + split;
+        const int cr = (hi == split + 1) ? leaf_base + split + 1 : node_base + split + 1;
+        BvhNodeTraverse* nt = tr + node;
+        nt->child_left = cl;
+        nt->child_right = cr;
+        nt->range_end = off + j;
+        if (lo == split) leaf_parent[off + split] = node;
+        else bd[cl].parent = node;
+        if (hi == split + 1) leaf_parent[off + split + 1] = node;
+        else bd[cr].parent = node;
+        bd[node].flag = 0;
+        if (i == 0) bd[node].parent = -1;       // segment root
+    }
+}
+
+struct ChildData {
+    float3 lo, hi, com;
+    float m;
+    double3 mx;   // FP64 mass-weighted position sums
+    double md;    // FP64 mass sum
+};
+
+__device__ __forceinline__ ChildData load_child(int c, int n_internal, const float4* __restrict__ pos,
+                                                const BvhNodeTraverse* tr, const BvhNodeBuild* bd,
+                                                const double4* com64, bool fp64) {
+    ChildData r;
+    if (c >= n_internal) {
+        const float4 p = __ldg(pos + (c - n_internal));
+        r.lo = r.hi = r.com = make_float3(p.x, p.y, p.z);
+        r.m = p.w;
+        if (fp64) {
+            r.md = p.w;
+            r.mx = make_double3((double)p.w * p.x, (double)p.w * p.y, (double)p.w * p.z);
+        }
+    } else {
+        // Written by another thread of this launch: read through L2.
+        const float4 a = __ldcg(reinterpret_cast<const float4*>(tr + c));
+        const float4 b0 = __ldcg(reinterpret_cast<const float4*>(bd + c));
+        const float2 b1 = __ldcg(reinterpret_cast<const float2*>(bd + c) + 2);
+        r.com = make_float3(a.x, a.y, a.z);
+        r.m = a.w;
+        r.lo = make_float3(b0.x, b0.y, b0.z);
+        r.hi = make_float3(b0.w, b1.x, b1.y);
+        if (fp64) {
+            const double2 q0 = __ldcg(reinterpret_cast<const double2*>(com64 + c));
+            const double2 q1 = __ldcg(reinterpret_cast<const double2*>(com64 + c) + 1);
+            r.mx = make_double3(q0.x, q0.y, q1.x);
+            r.md = q1.y;
+        }
+    }
+    return r;
+}
+
+__global__ void aggregate_kernel(Layout L, const float4* __restrict__ pos,
+                                 BvhNodeTraverse* __restrict__ tr, BvhNodeBuild* __restrict__ bd,
+                                 double4* __restrict__ com64, const int32_t* __restrict__ leaf_parent,
+                                 int com_fp64, uint32_t* __restrict__ status) {
+    const bool fp64 = com_fp64 != 0;
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < L.n; g += gridDim.x * blockDim.x) {
+        int node = __ldg(leaf_parent + g);
+        int levels = 0;
+        while (node >= 0) {
+            // a valid tree has at most 96 internal levels (strictly increasing
+            // prefix lengths below 96); more means malformed parent links
+            if (++levels > 96 || node >= L.n_internal) {
+                atomicOr(status, GCS_DEV_TREE_MALFORMED);
+                break;
+            }
+            __threadfence();
+            const int old = atomicAdd(&bd[node].flag, 1);
+            if (old == 0) break;                    // first arrival: the sibling finishes
+            __threadfence();
+            const int cl = __ldcg(&tr[node].child_left);
+            const int cr = __ldcg(&tr[node].child_right);
+            const ChildData A = load_child(cl, L.n_internal, pos, tr, bd, com64, fp64);
+            const ChildData B = load_child(cr, L.n_internal, pos, tr, bd, com64, fp64);
+            const float3 lo = make_float3(fminf(A.lo.x, B.lo.x), fminf(A.lo.y, B.lo.y),
+                                          fminf(A.lo.z, B.lo.z));
+            const float3 hi = make_float3(fmaxf(A.hi.x, B.hi.x), fmaxf(A.hi.y, B.hi.y),
+                                          fmaxf(A.hi.z, B.hi.z));
+            const float width = fmaxf(__fsub_rn(hi.x, lo.x),
+                                      fmaxf(__fsub_rn(hi.y, lo.y), __fsub_rn(hi.z, lo.z)));
+            const float m = __fadd_rn(A.m, B.m);
+            float3 com;
+            if (m > 0.0f) {
+                if (fp64) {
+                    const double md = A.md + B.md;
+                    const double3 mx = make_double3(A.mx.x + B.mx.x, A.mx.y + B.mx.y, A.mx.z + B.mx.z);
+                    com = make_float3((float)(mx.x / md), (float)(mx.y / md), (float)(mx.z / md));
+                    com64[node] = make_double4(mx.x, mx.y, mx.z, md);
+                } else {
+                    com = make_float3(com_fp32(A.com.x, A.m, B.com.x, B.m, m),
+                                      com_fp32(A.com.y, A.m, B.com.y, B.m, m),
+                                      com_fp32(A.com.z, A.m, B.com.z, B.m, m));
+                }
+            } else {
+                com = make_float3(__fmul_rn(__fadd_rn(lo.x, hi.x), 0.5f),
+                                  __fmul_rn(__fadd_rn(lo.y, hi.y), 0.5f),
+                                  __fmul_rn(__fadd_rn(lo.z, hi.z), 0.5f));
+                if (fp64) com64[node] = make_double4(0.0, 0.0, 0.0, 0.0);
+            }
+            float4* t4 = reinterpret_cast<float4*>(tr + node);
+            t4[0] = make_float4(com.x, com.y, com.z, m);
+            tr[node].width = width;
+            float4* b4 = reinterpret_cast<float4*>(bd + node);
+            b4[0] = make_float4(lo.x, lo.y, lo.z, hi.x);
+            reinterpret_cast<float2*>(b4 + 1)[0] = make_float2(hi.y, hi.z);
+            node = __ldcg(&bd[node].parent);
+        }
+    }
+}
+
+int tree_grid(int64_t n) {
+    int64_t b = (n + 255) / 256;
+    return (int)(b < 1 ? 1 : b);
+}
+
+}  // namespace
+
+void launch_build(const Layout& L, const uint64_t* keys, BvhNodeTraverse* tr, BvhNodeBuild* bd,
+                  int32_t* leaf_parent, uint32_t* status, cudaStream_t st) {
+    if (L.n <= 0) return;
+    build_kernel<<<tree_grid(L.n), 256, 0, st>>>(L, keys, tr, bd, leaf_parent, status);
+}
+
+void launch_aggregate(const Layout& L, const float4* pos, BvhNodeTraverse* tr, BvhNodeBuild* bd,
+                      double4* com64, const int32_t* leaf_parent, int com_fp64, uint32_t* status,
+                      cudaStream_t st) {
+    if (L.n <= 0) return;
+    aggregate_kernel<<<tree_grid(L.n), 256, 0, st>>>(L, pos, tr, bd, com64, leaf_parent, com_fp64, status);
+}
+
+}  // namespace gcs

@@ -1,0 +1,318 @@
+"""ctypes binding of libgcs.so (include/gcs.h) - the Python mirror of the
+engine's C ABI, used by the tests and bench.py.
+
+The engine is native code; this module only marshals arguments.  It raises
+if the library is missing or a call fails - there is no Python fallback.
+The record dtypes mirror include/gcs_types.h byte for byte.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgcs.so")
+
+STAR_DTYPE = np.dtype([("x", "<f4"), ("y", "<f4"), ("z", "<f4"), ("vx", "<f4"), ("vy", "<f4"),
+                       ("vz", "<f4"), ("mass", "<f4"), ("type", "u1"), ("r", "u1"), ("g", "u1"),
+                       ("b", "u1")])
+PLAYBACK_DTYPE = np.dtype([("x", "<f4"), ("y", "<f4"), ("z", "<f4"), ("r", "u1"), ("g", "u1"),
+                           ("b", "u1"), ("padding", "u1")])
+NODE_DTYPE = np.dtype([("com_x", "<f4"), ("com_y", "<f4"), ("com_z", "<f4"), ("mass", "<f4"),
+                       ("width", "<f4"), ("child_left", "<i4"), ("child_right", "<i4"),
+                       ("range_end", "<i4")])
+BUILD_DTYPE = np.dtype([("min_x", "<f4"), ("min_y", "<f4"), ("min_z", "<f4"), ("max_x", "<f4"),
+                        ("max_y", "<f4"), ("max_z", "<f4"), ("flag", "<i4"), ("parent", "<i4")])
+assert STAR_DTYPE.itemsize == 32 and PLAYBACK_DTYPE.itemsize == 16
+assert NODE_DTYPE.itemsize == 32 and BUILD_DTYPE.itemsize == 32
+
+OK = 0
+BOUNDS_CALLER, BOUNDS_DEVICE = 0, 1
+(STAGE_BOUNDS, STAGE_ENCODE, STAGE_SORT, STAGE_GATHER, STAGE_BUILD, STAGE_AGGREGATE, STAGE_WALK,
+ STAGE_INTEGRATE) = range(8)
+(BUF_KEYS, BUF_INDEX, BUF_NODES, BUF_BUILD, BUF_LEAF_PARENT, BUF_ACCEL, BUF_POS, BUF_VEL, BUF_BOUNDS,
+ BUF_KEYS_UNSORTED) = range(10)
+DEV_SORT_LOOKBACK_TIMEOUT, DEV_WALK_STACK_OVERFLOW, DEV_NONFINITE_POSITION, DEV_BUILD_RANGE = 1, 2, 4, 8
+DEV_TREE_MALFORMED = 16
+
+
+class Params(C.Structure):
+    _fields_ = [("G", C.c_float), ("epsilon_sq", C.c_float), ("theta", C.c_float), ("dt", C.c_float),
+                ("leaf_size", C.c_int32), ("bounds_mode", C.c_int32), ("global_min", C.c_float),
+                ("global_max", C.c_float), ("recolor", C.c_int32), ("com_fp64", C.c_int32),
+                ("walk_batch", C.c_int32), ("walk_blocks_per_sm", C.c_int32),
+                ("with_potential", C.c_int32), ("reserved", C.c_int32 * 3)]
+
+
+class GalaxySpec(C.Structure):
+    _fields_ = [("n_disc", C.c_int64), ("n_bulge", C.c_int64), ("n_halo", C.c_int64),
+                ("disc_mass", C.c_float), ("disc_a", C.c_float), ("disc_b", C.c_float),
+                ("disc_rmax", C.c_float), ("disc_zmax", C.c_float), ("bulge_mass", C.c_float),
+                ("bulge_a", C.c_float), ("bulge_rmax", C.c_float), ("halo_mass", C.c_float),
+                ("halo_a", C.c_float), ("halo_rmax", C.c_float), ("pos", C.c_float * 3),
+                ("vel", C.c_float * 3), ("incline_deg", C.c_float), ("type", C.c_uint8)]
+
+
+class CollisionSpec(C.Structure):
+    _fields_ = [("galaxy", GalaxySpec * 2), ("seed", C.c_uint64), ("G", C.c_float),
+                ("disc_dispersion", C.c_float)]
+
+
+class GcsError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load libgcs.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise GcsError("libgcs.so not built: run __graft_entry__.build() or make -C %s" % HERE)
+    L = C.CDLL(LIB_PATH)
+    P = C.c_void_p
+    i32, i64, u64, f32 = C.c_int32, C.c_int64, C.c_uint64, C.c_float
+    sig = {
+        "gcs_params_reference": (None, [C.POINTER(Params)]),
+        "gcs_create": (C.c_int, [C.POINTER(P), i64, i32, i32]),
+        "gcs_destroy": (None, [P]),
+        "gcs_set_stream": (C.c_int, [P, P]),
+        "gcs_get_stream": (P, [P]),
+        "gcs_status_string": (C.c_char_p, [C.c_int]),
+        "gcs_last_error": (C.c_char_p, [P]),
+        "gcs_set_segments": (C.c_int, [P, i32, C.POINTER(i64)]),
+        "gcs_num_particles": (i64, [P]),
+        "gcs_num_segments": (i32, [P]),
+        "gcs_num_internal_nodes": (i64, [P]),
+        "gcs_upload_stars": (C.c_int, [P, P, i64, i64]),
+        "gcs_download_stars": (C.c_int, [P, P, i64, i64]),
+        "gcs_download_playback": (C.c_int, [P, P, i64, i64]),
+        "gcs_step": (C.c_int, [P, C.POINTER(Params)]),
+        "gcs_step_host": (C.c_int, [P, C.POINTER(Params), P]),
+        "gcs_compute_accels": (C.c_int, [P, C.POINTER(Params)]),
+        "gcs_kick": (C.c_int, [P, f32]),
+        "gcs_run_stages": (C.c_int, [P, C.POINTER(Params), i32, i32]),
+        "gcs_synchronize": (C.c_int, [P]),
+        "gcs_device_status": (C.c_int, [P, C.POINTER(C.c_uint32), i32]),
+        "gcs_read_buffer": (C.c_int, [P, i32, P, i64, i64]),
+        "gcs_collision_spec_equal": (C.c_int, [C.POINTER(CollisionSpec), i64, i64, i64, u64]),
+        "gcs_collision_spec_pair": (C.c_int, [C.POINTER(CollisionSpec), i64, f32, f32, f32, f32, u64]),
+        "gcs_collision_count": (i64, [C.POINTER(CollisionSpec)]),
+        "gcs_generate_collision": (C.c_int, [C.POINTER(CollisionSpec), P, i64]),
+        "gcs_diagnostics": (C.c_int, [P, i32, C.POINTER(C.c_double)]),
+        "gcs_direct_accels_fp64": (C.c_int, [P, C.POINTER(Params), i32, C.POINTER(i64), i64,
+                                             C.POINTER(C.c_double)]),
+        "gcs_count_interactions": (C.c_int, [P, C.POINTER(Params), C.POINTER(C.c_uint64)]),
+        "gcs_dropin_set_params": (C.c_int, [C.POINTER(Params)]),
+        "gcs_dropin_context": (P, []),
+        "gcs_dropin_device_stars": (P, []),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def _ptr(a: np.ndarray) -> C.c_void_p:
+    assert a.flags["C_CONTIGUOUS"]
+    return C.c_void_p(a.ctypes.data)
+
+
+def reference_params(**kw) -> Params:
+    p = Params()
+    lib().gcs_params_reference(C.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def collision_equal(n_disc: int, n_bulge: int, n_halo: int, seed: int = 0) -> np.ndarray:
+    """The equal-galaxy recipe (per-galaxy counts given) as a Star array."""
+    spec = CollisionSpec()
+    _check(lib().gcs_collision_spec_equal(C.byref(spec), n_disc, n_bulge, n_halo, seed), None)
+    return _generate(spec)
+
+
+def collision_pair(n_total: int, q: float, impact: float, rel_speed: float, incline_deg: float,
+                   seed: int) -> np.ndarray:
+    spec = CollisionSpec()
+    _check(lib().gcs_collision_spec_pair(C.byref(spec), n_total, q, impact, rel_speed, incline_deg, seed),
+           None)
+    return _generate(spec)
+
+
+def _generate(spec: CollisionSpec) -> np.ndarray:
+    n = lib().gcs_collision_count(C.byref(spec))
+    out = np.zeros(n, dtype=STAR_DTYPE)
+    _check(lib().gcs_generate_collision(C.byref(spec), _ptr(out), n), None)
+    return out
+
+
+def _check(rc: int, ctx) -> None:
+    if rc != OK:
+        L = lib()
+        msg = L.gcs_status_string(rc).decode()
+        if ctx is not None:
+            msg += ": " + (L.gcs_last_error(ctx) or b"").decode()
+        raise GcsError("gcs call failed (%d): %s" % (rc, msg))
+
+
+# The two configs the recipe names by count.
+SMALL_COUNTS = (16384, 4096, 2048)       # 45,056 particles
+LARGE_COUNTS = (384000, 96000, 44288)    # 1,048,576 particles
+
+
+class Context:
+    """One gcs_ctx: device state for up to `capacity` particles."""
+
+    def __init__(self, capacity: int, max_segments: int = 1, device: int = 0):
+        self._h = C.c_void_p()
+        self.L = lib()
+        rc = self.L.gcs_create(C.byref(self._h), capacity, max_segments, device)
+        if rc != OK:
+            raise GcsError("gcs_create failed: %s" % self.L.gcs_status_string(rc).decode())
+        self.capacity = capacity
+
+    def close(self) -> None:
+        if self._h:
+            self.L.gcs_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    def check(self, rc: int) -> None:
+        _check(rc, self._h)
+
+    def set_stream(self, stream_ptr: int) -> None:
+        self.check(self.L.gcs_set_stream(self._h, C.c_void_p(stream_ptr)))
+
+    def set_segments(self, counts) -> None:
+        arr = (C.c_int64 * len(counts))(*[int(c) for c in counts])
+        self.check(self.L.gcs_set_segments(self._h, len(counts), arr))
+
+    @property
+    def n(self) -> int:
+        return int(self.L.gcs_num_particles(self._h))
+
+    @property
+    def n_internal(self) -> int:
+        return int(self.L.gcs_num_internal_nodes(self._h))
+
+    def upload(self, stars: np.ndarray, offset: int = 0) -> None:
+        stars = np.ascontiguousarray(stars, dtype=STAR_DTYPE)
+        self.check(self.L.gcs_upload_stars(self._h, _ptr(stars), offset, len(stars)))
+
+    def download(self, offset: int = 0, n: int | None = None, out: np.ndarray | None = None) -> np.ndarray:
+        n = self.n - offset if n is None else n
+        out = np.zeros(n, dtype=STAR_DTYPE) if out is None else out
+        self.check(self.L.gcs_download_stars(self._h, _ptr(out), offset, n))
+        return out
+
+    def download_playback(self, offset: int = 0, n: int | None = None) -> np.ndarray:
+        n = self.n - offset if n is None else n
+        out = np.zeros(n, dtype=PLAYBACK_DTYPE)
+        self.check(self.L.gcs_download_playback(self._h, _ptr(out), offset, n))
+        return out
+
+    def step(self, p: Params) -> None:
+        self.check(self.L.gcs_step(self._h, C.byref(p)))
+
+    def step_host(self, p: Params, out: np.ndarray) -> None:
+        self.check(self.L.gcs_step_host(self._h, C.byref(p), _ptr(out)))
+
+    def compute_accels(self, p: Params) -> None:
+        self.check(self.L.gcs_compute_accels(self._h, C.byref(p)))
+
+    def kick(self, dt: float) -> None:
+        self.check(self.L.gcs_kick(self._h, dt))
+
+    def run_stages(self, p: Params, first: int, last: int) -> None:
+        self.check(self.L.gcs_run_stages(self._h, C.byref(p), first, last))
+
+    def synchronize(self) -> None:
+        self.check(self.L.gcs_synchronize(self._h))
+
+    def device_status(self, clear: bool = False) -> int:
+        s = C.c_uint32()
+        self.check(self.L.gcs_device_status(self._h, C.byref(s), int(clear)))
+        return int(s.value)
+
+    _BUF = {BUF_KEYS: ("<u8", 1), BUF_INDEX: ("<u4", 1), BUF_NODES: (NODE_DTYPE, 1),
+            BUF_BUILD: (BUILD_DTYPE, 1), BUF_LEAF_PARENT: ("<i4", 1), BUF_ACCEL: ("<f4", 4),
+            BUF_POS: ("<f4", 4), BUF_VEL: ("<f4", 4), BUF_BOUNDS: ("<f4", 2),
+            BUF_KEYS_UNSORTED: ("<u8", 1)}
+
+    def read(self, which: int, first: int = 0, count: int | None = None) -> np.ndarray:
+        dt, width = self._BUF[which]
+        if count is None:
+            limit = {BUF_NODES: self.n_internal, BUF_BUILD: self.n_internal,
+                     BUF_BOUNDS: int(self.L.gcs_num_segments(self._h))}.get(which, self.n)
+            count = limit - first
+        shape = (count, width) if width > 1 else (count,)
+        out = np.zeros(shape, dtype=dt)
+        self.check(self.L.gcs_read_buffer(self._h, which, _ptr(out), first, count))
+        return out
+
+    def diagnostics(self, segment: int = 0) -> np.ndarray:
+        out = (C.c_double * 6)()
+        self.check(self.L.gcs_diagnostics(self._h, segment, out))
+        return np.array(out[:])
+
+    def count_interactions(self, p: Params) -> tuple[int, int]:
+        out = (C.c_uint64 * 2)()
+        self.check(self.L.gcs_count_interactions(self._h, C.byref(p), out))
+        return int(out[0]), int(out[1])
+
+    def direct_fp64(self, p: Params, targets, segment: int = 0) -> np.ndarray:
+        t = np.ascontiguousarray(targets, dtype=np.int64)
+        out = np.zeros((len(t), 3), dtype=np.float64)
+        self.check(self.L.gcs_direct_accels_fp64(
+            self._h, C.byref(p), segment, t.ctypes.data_as(C.POINTER(C.c_int64)), len(t),
+            out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
+
+def pos_vel_from_stars(stars: np.ndarray):
+    """Split Stars into the engine's (x,y,z,m) and (vx,vy,vz,tcol-bits) float4 rows."""
+    n = len(stars)
+    pos = np.zeros((n, 4), np.float32)
+    vel = np.zeros((n, 4), np.float32)
+    pos[:, 0], pos[:, 1], pos[:, 2], pos[:, 3] = stars["x"], stars["y"], stars["z"], stars["mass"]
+    vel[:, 0], vel[:, 1], vel[:, 2] = stars["vx"], stars["vy"], stars["vz"]
+    tcol = (stars["type"].astype(np.uint32) | (stars["r"].astype(np.uint32) << 8)
+            | (stars["g"].astype(np.uint32) << 16) | (stars["b"].astype(np.uint32) << 24))
+    vel[:, 3] = tcol.view(np.float32)
+    return pos, vel
+
+
+def stars_from_pos_vel(pos: np.ndarray, vel: np.ndarray) -> np.ndarray:
+    out = np.zeros(len(pos), dtype=STAR_DTYPE)
+    out["x"], out["y"], out["z"], out["mass"] = pos[:, 0], pos[:, 1], pos[:, 2], pos[:, 3]
+    out["vx"], out["vy"], out["vz"] = vel[:, 0], vel[:, 1], vel[:, 2]
+    tcol = np.ascontiguousarray(vel[:, 3]).view(np.uint32)
+    out["type"] = tcol & 0xFF
+    out["r"] = (tcol >> 8) & 0xFF
+    out["g"] = (tcol >> 16) & 0xFF
+    out["b"] = (tcol >> 24) & 0xFF
+    return out

@@ -1,0 +1,232 @@
+/*
+ * gcs.h - C ABI of the B200 Barnes-Hut engine ("gcs" = galaxy collision
+ * simulator).
+ *
+ * This is the boundary a foreign caller binds (ctypes, cgo, JNI ...).  The
+ * reference exposes its GPU engine as C++ functions over file-scope globals
+ * (cuda_engine.h:5-32 of lakshya076/Galaxy-Collision-Simulator); those exact
+ * C++ signatures are kept in include/cuda_engine.h as thin wrappers over the
+ * context API below.  Everything here is extern "C", takes plain pointers and
+ * sizes, and reports failure through an int status (GCS_OK == 0).
+ *
+ * One context owns one device's state: the particle arrays of one or more
+ * segments (independent scenarios laid out back to back), the tree, the sort
+ * buffers and the per-step scratch.  All work is queued on the context's
+ * stream; calls that return host data synchronise that stream.
+ *
+ * Per step, for every segment, the engine runs the reference's pipeline
+ * (cuda_engine.cu:379-451): bounds -> 63-bit Morton encode -> stable radix
+ * sort with index tie-break -> gather -> Karras build -> bottom-up
+ * aggregation -> tree walk -> kick+drift (+ colour) -> optional pack.
+ */
+#ifndef GCS_H
+#define GCS_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include "gcs_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define GCS_OK            0
+#define GCS_ERR_ARG      -1  /* bad argument (null, size out of range, ...) */
+#define GCS_ERR_CUDA     -2  /* a CUDA runtime call failed */
+#define GCS_ERR_NOMEM    -3  /* device or host allocation failed */
+#define GCS_ERR_CAPACITY -4  /* more particles/segments than the context holds */
+#define GCS_ERR_DEVICE   -5  /* a kernel raised a bit of the device status word */
+#define GCS_ERR_STATE    -6  /* call not valid in the context's current state */
+#define GCS_ERR_NO_DEVICE -7 /* no CUDA device, or not an sm_100 device */
+
+/* Bits of the device status word (gcs_device_status).  Kernels never trap:
+ * a bounded wait that runs out, or a capacity that would be exceeded, sets a
+ * bit, skips the offending access and returns. */
+#define GCS_DEV_SORT_LOOKBACK_TIMEOUT 0x1u /* radix-sort decoupled look-back gave up */
+#define GCS_DEV_WALK_STACK_OVERFLOW   0x2u /* a walk stack would have overflowed */
+#define GCS_DEV_NONFINITE_POSITION    0x4u /* NaN/Inf position met in bounds/encode */
+#define GCS_DEV_BUILD_RANGE           0x8u /* Karras build produced an out-of-range child */
+#define GCS_DEV_TREE_MALFORMED        0x10u /* a walk or climb exceeded the bound a valid tree obeys */
+
+/* ---- step parameters --------------------------------------------------- */
+#define GCS_BOUNDS_CALLER 0 /* use global_min/global_max for every segment (reference API) */
+#define GCS_BOUNDS_DEVICE 1 /* per-segment min/max reduced on the device */
+
+typedef struct gcs_params {
+    float G;            /* gravitational constant (reference passes 1) */
+    float epsilon_sq;   /* Plummer softening eps^2, added to every d^2 */
+    float theta;        /* opening angle: a node is used as a monopole when
+                           width^2 < theta^2 * (d^2 + eps^2); the reference's
+                           GPU walk is theta = 1 (cuda_engine.cu:143) */
+    float dt;           /* kick+drift step */
+    int32_t leaf_size;  /* L >= 1: an opened node holding <= L particles is
+                           summed particle by particle (reference: 1) */
+    int32_t bounds_mode;/* GCS_BOUNDS_CALLER or GCS_BOUNDS_DEVICE */
+    float global_min;   /* Morton cube, used with GCS_BOUNDS_CALLER */
+    float global_max;
+    int32_t recolor;    /* 1: the reference's speed colour map for types 0/2 */
+    int32_t com_fp64;   /* 1: node centres of mass from FP64 sums;
+                           0: the reference's FP32 pairwise formula */
+    int32_t walk_batch; /* nodes fetched per stack pop, 1..32 (0 = tuned default) */
+    int32_t walk_blocks_per_sm; /* persistent walk occupancy (0 = default) */
+    int32_t with_potential; /* 1: the walk also sums potentials (ACCEL .w) */
+    int32_t reserved[3];
+} gcs_params;
+
+/* The reference's fixed settings: G=1, eps^2=10, theta=1, dt=0.01, L=1,
+ * caller bounds [-1e4, 1e4] (main.cpp:111-112,197,461-462), FP32 COM,
+ * recolouring on. */
+void gcs_params_reference(gcs_params* p);
+
+/* ---- context lifecycle -------------------------------------------------- */
+typedef struct gcs_ctx gcs_ctx;
+
+/* Allocates device state for up to `capacity` particles in up to
+ * `max_segments` segments on `device`.  The context starts with one segment
+ * of `capacity` particles. */
+int gcs_create(gcs_ctx** out, int64_t capacity, int32_t max_segments, int32_t device);
+void gcs_destroy(gcs_ctx* ctx);
+/* Queue all further work on `stream` (a cudaStream_t; NULL = the legacy
+ * default stream).  The caller keeps the stream alive. */
+int gcs_set_stream(gcs_ctx* ctx, void* stream);
+void* gcs_get_stream(const gcs_ctx* ctx);
+const char* gcs_status_string(int status);
+/* Text of the last failure on this context ("" if none). */
+const char* gcs_last_error(const gcs_ctx* ctx);
+
+/* ---- layout --------------------------------------------------------------
+ * Segments are independent scenarios packed back to back: segment s holds
+ * particles [off_s, off_s + counts[s]).  Changing the layout invalidates the
+ * particle data. */
+int gcs_set_segments(gcs_ctx* ctx, int32_t num_segments, const int64_t* counts);
+int64_t gcs_num_particles(const gcs_ctx* ctx);
+int32_t gcs_num_segments(const gcs_ctx* ctx);
+
+/* ---- particle data ------------------------------------------------------ */
+/* Copy host Stars into particles [offset, offset+n) (host may be pageable or
+ * pinned); the reference's cuda_upload_initial_stars (cuda_engine.cu:342-352). */
+int gcs_upload_stars(gcs_ctx* ctx, const Star* host, int64_t offset, int64_t n);
+/* Pack particles [offset, offset+n) as Stars and copy them to host; synchronises. */
+int gcs_download_stars(gcs_ctx* ctx, Star* host, int64_t offset, int64_t n);
+/* Pack particles [offset, offset+n) as simulation.bin records and copy to
+ * host; synchronises. */
+int gcs_download_playback(gcs_ctx* ctx, PlaybackStar* host, int64_t offset, int64_t n);
+
+/* ---- stepping ----------------------------------------------------------- */
+/* One full step of every segment, queued on the context stream. */
+int gcs_step(gcs_ctx* ctx, const gcs_params* p);
+/* One step, then pack every particle as Star into `host` (pinned for an
+ * asynchronous-capable copy) and synchronise: the reference's
+ * cuda_physics_step with use_interop=false (cuda_engine.cu:379-451). */
+int gcs_step_host(gcs_ctx* ctx, const gcs_params* p, Star* host);
+/* Accelerations at the current positions (bounds..walk, no kick/drift).
+ * Afterwards the particle arrays are in this step's Morton order and the
+ * acceleration buffer matches them. */
+int gcs_compute_accels(gcs_ctx* ctx, const gcs_params* p);
+/* v += a * dt with the last computed accelerations (a half-kick for
+ * kick-drift-kick open/close). */
+int gcs_kick(gcs_ctx* ctx, float dt);
+
+/* Pipeline stages, for stage-by-stage checking.  gcs_run_stages runs
+ * stages first..last inclusive with the given parameters. */
+#define GCS_STAGE_BOUNDS    0
+#define GCS_STAGE_ENCODE    1
+#define GCS_STAGE_SORT      2
+#define GCS_STAGE_GATHER    3
+#define GCS_STAGE_BUILD     4
+#define GCS_STAGE_AGGREGATE 5
+#define GCS_STAGE_WALK      6
+#define GCS_STAGE_INTEGRATE 7
+int gcs_run_stages(gcs_ctx* ctx, const gcs_params* p, int32_t first, int32_t last);
+
+/* Wait for the context stream; returns GCS_ERR_DEVICE if the device status
+ * word is non-zero (read it with gcs_device_status). */
+int gcs_synchronize(gcs_ctx* ctx);
+/* Device status word (GCS_DEV_* bits), synchronising; `clear` resets it. */
+int gcs_device_status(gcs_ctx* ctx, uint32_t* status, int32_t clear);
+
+/* ---- introspection (synchronises) ----------------------------------------
+ * Copy `count` elements starting at element `first` of an internal buffer to
+ * host.  Element types: KEYS u64, INDEX u32 (sorted position -> position
+ * before this step's sort), NODES BvhNodeTraverse, BUILD BvhNodeBuild,
+ * LEAF_PARENT i32, ACCEL float4 (ax,ay,az,potential), POS float4 (x,y,z,m),
+ * VEL float4 (vx,vy,vz, bits of type|r|g|b), BOUNDS float2 per segment,
+ * KEYS_UNSORTED u64 (encode output). */
+#define GCS_BUF_KEYS          0
+#define GCS_BUF_INDEX         1
+#define GCS_BUF_NODES         2
+#define GCS_BUF_BUILD         3
+#define GCS_BUF_LEAF_PARENT   4
+#define GCS_BUF_ACCEL         5
+#define GCS_BUF_POS           6
+#define GCS_BUF_VEL           7
+#define GCS_BUF_BOUNDS        8
+#define GCS_BUF_KEYS_UNSORTED 9
+int gcs_read_buffer(gcs_ctx* ctx, int32_t which, void* host, int64_t first, int64_t count);
+/* Number of internal tree nodes (sum over segments of count-1). */
+int64_t gcs_num_internal_nodes(const gcs_ctx* ctx);
+
+/* ---- initial conditions -------------------------------------------------
+ * Seeded two-galaxy collision: each galaxy is a Miyamoto-Nagai disc, a
+ * Hernquist bulge and a Hernquist dark-matter halo (the reference's
+ * generator.cpp:3-196 components), with the recipe's masses, scale lengths,
+ * truncations and orbit given here.  Deterministic for a given spec. */
+typedef struct gcs_galaxy_spec {
+    int64_t n_disc, n_bulge, n_halo;
+    float disc_mass, disc_a, disc_b, disc_rmax, disc_zmax;
+    float bulge_mass, bulge_a, bulge_rmax;
+    float halo_mass, halo_a, halo_rmax;
+    float pos[3], vel[3];
+    float incline_deg;   /* rotation of the whole galaxy about the x axis */
+    uint8_t type;        /* 0 = galaxy A colours, 2 = galaxy B colours */
+} gcs_galaxy_spec;
+
+typedef struct gcs_collision_spec {
+    gcs_galaxy_spec galaxy[2];
+    uint64_t seed;
+    float G;
+    float disc_dispersion; /* disc velocity noise, fraction of v_c */
+} gcs_collision_spec;
+
+/* Equal galaxies (the recipe of the 45,056- and 1,048,576-particle cases):
+ * disc a=3, b=0.3, M=1 (R<=15, |z|<=3); bulge a=0.5, M=0.33 (r<=5); halo
+ * a=10, M=5.8 (r<=30); galaxy A at (-20,-5,0) moving (+0.4,0,0), galaxy B at
+ * (+20,+5,0) moving (-0.4,0,0) with its disc inclined 30 deg about x.
+ * Per-galaxy counts are given (16384/4096/2048 and 384000/96000/44288 in
+ * the two cases). */
+int gcs_collision_spec_equal(gcs_collision_spec* spec, int64_t n_disc, int64_t n_bulge,
+                             int64_t n_halo, uint64_t seed);
+/* Unequal pair: galaxy B is the equal-case galaxy, galaxy A is it scaled to
+ * mass ratio q = M_A/M_B in (0,1] (lengths by q^(1/3)); impact parameter b
+ * along y, relative speed v along x, 40 length units apart in x, centre of
+ * mass at rest at the origin; galaxy B inclined by incline_deg.  Particle
+ * counts are proportional to mass (equal particle masses across galaxies),
+ * split disc:bulge:halo as 384000:96000:44288. */
+int gcs_collision_spec_pair(gcs_collision_spec* spec, int64_t n_total, float q,
+                            float impact, float rel_speed, float incline_deg,
+                            uint64_t seed);
+int64_t gcs_collision_count(const gcs_collision_spec* spec);
+int gcs_generate_collision(const gcs_collision_spec* spec, Star* out, int64_t n);
+
+/* ---- diagnostics --------------------------------------------------------
+ * FP64 reductions over one segment's current state: out = {kinetic energy,
+ * px, py, pz, total mass, potential energy}.  The potential energy is
+ * 0.5 * sum m_i phi_i over the potentials of the last walk, which must have
+ * run with with_potential = 1 at the current positions (else it is 0). */
+int gcs_diagnostics(gcs_ctx* ctx, int32_t segment, double out[6]);
+/* Interaction counts of one walk at the current state: runs bounds..walk
+ * with the counting walk and returns {monopole terms, particle terms}
+ * summed over all targets (the unit of interactions/s; 20 FP32 flops each). */
+int gcs_count_interactions(gcs_ctx* ctx, const gcs_params* p, uint64_t out[2]);
+/* FP64 direct-sum accelerations (excluding only i == j) at `n_targets`
+ * sorted positions `targets` of one segment; result as double[3*n_targets].
+ * Reads the current positions; eps^2 and G from p. */
+int gcs_direct_accels_fp64(gcs_ctx* ctx, const gcs_params* p, int32_t segment,
+                           const int64_t* targets, int64_t n_targets, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GCS_H */

@@ -1,0 +1,314 @@
+"""GPU parity: every stage of the CUDA path against the oracle on the same
+seeded inputs, called through the C ABI.
+
+Bars: bit-exact for keys, permutation, topology, bounds, masses, widths and
+the integrate step (same inputs); accelerations within 1e-5 relative
+(FP32 reassociation and rsqrtf vs IEEE 1/sqrt only), measured per particle
+as |a - a_ref| / max(|a_ref|, 1e-3 * median |a_ref|), required at the 99.9th
+percentile, with 1e-4 as the per-particle maximum."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from conftest import rel_err, small_collision
+
+pytestmark = pytest.mark.gpu
+
+TOL_ACC = 1e-5
+TOL_ACC_MAX = 1e-4
+
+
+def _acc_err(a, ref):
+    scale = np.median(np.linalg.norm(ref, axis=1))
+    return rel_err(a, ref, floor=1e-3 * scale)
+
+
+def _assert_acc(a, ref, what=""):
+    e = _acc_err(a, ref)
+    assert np.percentile(e, 99.9) <= TOL_ACC, (what, np.percentile(e, 99.9))
+    assert e.max() <= TOL_ACC_MAX, (what, e.max())
+
+
+@pytest.fixture(scope="module")
+def stars():
+    return small_collision(2048, 512, 256, seed=11)  # 5632 particles
+
+
+def _params(gcs, **kw):
+    p = gcs.reference_params(bounds_mode=gcs.BOUNDS_DEVICE, theta=0.5, epsilon_sq=0.05 ** 2, dt=0.005,
+                             leaf_size=1)
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def _ctx(gcs, stars, segments=None):
+    n = len(stars)
+    ctx = gcs.Context(n, max_segments=len(segments) if segments else 1)
+    ctx.set_segments(segments or [n])
+    ctx.upload(stars)
+    return ctx
+
+
+def test_bounds_and_encode_bitexact(gcs_mod, oracle_mod, stars):
+    gcs = gcs_mod
+    pos, _ = gcs.pos_vel_from_stars(stars)
+    with _ctx(gcs, stars) as ctx:
+        p = _params(gcs)
+        ctx.run_stages(p, gcs.STAGE_BOUNDS, gcs.STAGE_ENCODE)
+        lo, hi = oracle_mod.bounds(pos)
+        np.testing.assert_array_equal(ctx.read(gcs.BUF_BOUNDS)[0], [lo, hi])
+        np.testing.assert_array_equal(ctx.read(gcs.BUF_KEYS_UNSORTED), oracle_mod.encode(pos, lo, hi))
+        # caller bounds (the reference API), including particles outside the cube
+        p = _params(gcs, bounds_mode=gcs.BOUNDS_CALLER, global_min=-30.0, global_max=20.0)
+        ctx.run_stages(p, gcs.STAGE_BOUNDS, gcs.STAGE_ENCODE)
+        np.testing.assert_array_equal(ctx.read(gcs.BUF_KEYS_UNSORTED),
+                                      oracle_mod.encode(pos, np.float32(-30.0), np.float32(20.0)))
+        assert ctx.device_status() == 0
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 4095, 4096, 4097, 70001])
+def test_sort_bitexact(gcs_mod, oracle_mod, n):
+    gcs = gcs_mod
+    st = small_collision(max(n // 2, 1), 0, 0, seed=n)[:n]
+    if len(st) < n:
+        st = np.resize(st, n)
+    rng = np.random.default_rng(n)
+    if n > 10:  # force duplicate keys
+        st["x"][: n // 3] = st["x"][0]
+        st["y"][: n // 3] = st["y"][0]
+        st["z"][: n // 3] = st["z"][0]
+    st["x"] += rng.normal(0, 1e-3, n).astype(np.float32) * (rng.random(n) < 0.5)
+    pos, _ = gcs.pos_vel_from_stars(st)
+    with _ctx(gcs, st) as ctx:
+        p = _params(gcs)
+        ctx.run_stages(p, gcs.STAGE_BOUNDS, gcs.STAGE_SORT)
+        lo, hi = oracle_mod.bounds(pos)
+        sk, idx = oracle_mod.sort(oracle_mod.encode(pos, lo, hi))
+        np.testing.assert_array_equal(ctx.read(gcs.BUF_KEYS), sk)
+        np.testing.assert_array_equal(ctx.read(gcs.BUF_INDEX), idx)
+        assert ctx.device_status() == 0
+
+
+def test_build_topology_bitexact(gcs_mod, oracle_mod, stars):
+    gcs = gcs_mod
+    pos, _ = gcs.pos_vel_from_stars(stars)
+    n = len(stars)
+    with _ctx(gcs, stars) as ctx:
+        ctx.run_stages(_params(gcs), gcs.STAGE_BOUNDS, gcs.STAGE_BUILD)
+        lo, hi = oracle_mod.bounds(pos)
+        sk, _ = oracle_mod.sort(oracle_mod.encode(pos, lo, hi))
+        cl, cr, re, par, lp = oracle_mod.build(sk)
+        nodes = ctx.read(gcs.BUF_NODES)
+        np.testing.assert_array_equal(nodes["child_left"], cl)
+        np.testing.assert_array_equal(nodes["child_right"], cr)
+        np.testing.assert_array_equal(nodes["range_end"], re)
+        np.testing.assert_array_equal(ctx.read(gcs.BUF_BUILD)["parent"], par)
+        np.testing.assert_array_equal(ctx.read(gcs.BUF_LEAF_PARENT), lp)
+        assert ctx.n_internal == n - 1
+        assert ctx.device_status() == 0
+
+
+@pytest.mark.parametrize("com_fp64", [0, 1])
+def test_aggregate(gcs_mod, oracle_mod, stars, com_fp64):
+    gcs = gcs_mod
+    with _ctx(gcs, stars) as ctx:
+        ctx.run_stages(_params(gcs, com_fp64=com_fp64), gcs.STAGE_BOUNDS, gcs.STAGE_AGGREGATE)
+        sp = ctx.read(gcs.BUF_POS)
+        nodes = ctx.read(gcs.BUF_NODES)
+        bd = ctx.read(gcs.BUF_BUILD)
+        ref, box = oracle_mod.aggregate(sp, nodes["child_left"], nodes["child_right"], nodes["range_end"],
+                                        com_fp64=bool(com_fp64))
+        np.testing.assert_array_equal(nodes["mass"], ref["mass"])
+        np.testing.assert_array_equal(nodes["width"], ref["width"])
+        np.testing.assert_array_equal(np.stack([bd["min_x"], bd["min_y"], bd["min_z"]], 1), box[:, :3])
+        np.testing.assert_array_equal(np.stack([bd["max_x"], bd["max_y"], bd["max_z"]], 1), box[:, 3:])
+        for a in ("com_x", "com_y", "com_z"):
+            np.testing.assert_array_equal(nodes[a], ref[a], err_msg=a)
+
+
+@pytest.mark.parametrize("theta,leaf", [(1.0, 1), (0.5, 1), (0.5, 8), (0.5, 32), (0.7, 16), (0.0, 4)])
+def test_walk_matches_oracle(gcs_mod, oracle_mod, stars, theta, leaf):
+    gcs = gcs_mod
+    with _ctx(gcs, stars) as ctx:
+        p = _params(gcs, theta=theta, leaf_size=leaf, with_potential=1)
+        ctx.run_stages(p, gcs.STAGE_BOUNDS, gcs.STAGE_WALK)
+        sp = ctx.read(gcs.BUF_POS)
+        nodes = ctx.read(gcs.BUF_NODES)
+        acc = ctx.read(gcs.BUF_ACCEL)
+        ref = oracle_mod.walk(sp, nodes, p.G, p.epsilon_sq, theta, leaf)
+        _assert_acc(acc[:, :3], ref[:, :3], "theta=%s L=%s" % (theta, leaf))
+        np.testing.assert_allclose(acc[:, 3], ref[:, 3], rtol=1e-5)
+        assert ctx.device_status() == 0
+
+
+@pytest.mark.parametrize("batch", [1, 4, 32])
+def test_walk_batch_sizes_agree(gcs_mod, stars, batch):
+    gcs = gcs_mod
+    with _ctx(gcs, stars) as ctx:
+        ctx.run_stages(_params(gcs, walk_batch=1, leaf_size=8), gcs.STAGE_BOUNDS, gcs.STAGE_WALK)
+        a1 = ctx.read(gcs.BUF_ACCEL)
+        ctx.run_stages(_params(gcs, walk_batch=batch, leaf_size=8), gcs.STAGE_WALK, gcs.STAGE_WALK)
+        a2 = ctx.read(gcs.BUF_ACCEL)
+        _assert_acc(a2[:, :3], a1[:, :3])
+
+
+def test_integrate_bitexact(gcs_mod, oracle_mod, stars):
+    gcs = gcs_mod
+    with _ctx(gcs, stars) as ctx:
+        # large speeds so the colour map crosses both branches
+        s2 = stars.copy()
+        rng = np.random.default_rng(3)
+        s2["vx"] = rng.uniform(-200, 200, len(s2)).astype(np.float32)
+        ctx.upload(s2)
+        p = _params(gcs, dt=0.01)
+        ctx.run_stages(p, gcs.STAGE_BOUNDS, gcs.STAGE_WALK)
+        x0, v0, a = ctx.read(gcs.BUF_POS), ctx.read(gcs.BUF_VEL), ctx.read(gcs.BUF_ACCEL)
+        ctx.run_stages(p, gcs.STAGE_INTEGRATE, gcs.STAGE_INTEGRATE)
+        x1, v1 = ctx.read(gcs.BUF_POS), ctx.read(gcs.BUF_VEL)
+        xr, vr = oracle_mod.integrate(x0, v0, a, p.dt, True)
+        np.testing.assert_array_equal(x1, xr)
+        np.testing.assert_array_equal(v1.view(np.uint32), vr.view(np.uint32))
+
+
+def test_full_step_matches_oracle_step(gcs_mod, oracle_mod, stars):
+    gcs = gcs_mod
+    pos, vel = gcs.pos_vel_from_stars(stars)
+    for leaf in (1, 16):
+        with _ctx(gcs, stars) as ctx:
+            p = _params(gcs, leaf_size=leaf)
+            ctx.step(p)
+            out = ctx.download()
+            acc = ctx.read(gcs.BUF_ACCEL)
+            xr, vr, ar, _ = oracle_mod.step(pos, vel, p.G, p.epsilon_sq, p.theta, leaf, p.dt)
+            sr = gcs.stars_from_pos_vel(xr, vr)
+            _assert_acc(acc[:, :3], ar[:, :3], "step L=%d" % leaf)
+            for f in ("mass", "type"):
+                np.testing.assert_array_equal(out[f], sr[f])
+            for f in ("x", "y", "z", "vx", "vy", "vz"):
+                np.testing.assert_allclose(out[f], sr[f], rtol=1e-6, atol=1e-6)
+            assert ctx.device_status() == 0
+
+
+def test_segments_match_solo_bitwise(gcs_mod, stars):
+    """Scenarios batched as segments give exactly their solo results."""
+    gcs = gcs_mod
+    a = stars[:1]
+    b = stars[1:3]
+    c = small_collision(300, 100, 77, seed=5)
+    d = stars[3:3 + 4101]
+    parts = [a, b, c, d]
+    allst = np.concatenate(parts)
+    p = _params(gcs, leaf_size=8)
+    with _ctx(gcs, allst, segments=[len(x) for x in parts]) as ctx:
+        for _ in range(3):
+            ctx.step(p)
+        batched = ctx.download()
+        bacc = ctx.read(gcs.BUF_ACCEL)
+        assert ctx.device_status() == 0
+    off = 0
+    for part in parts:
+        with _ctx(gcs, part) as solo:
+            for _ in range(3):
+                solo.step(p)
+            np.testing.assert_array_equal(solo.download().tobytes(), batched[off:off + len(part)].tobytes())
+            np.testing.assert_array_equal(solo.read(gcs.BUF_ACCEL), bacc[off:off + len(part)])
+        off += len(part)
+
+
+def test_edge_cases(gcs_mod, oracle_mod):
+    gcs = gcs_mod
+    st = small_collision(64, 16, 8, seed=2)
+    # one particle: no force
+    with _ctx(gcs, st[:1]) as ctx:
+        ctx.step(_params(gcs))
+        assert np.all(ctx.read(gcs.BUF_ACCEL) == 0)
+    # every particle at one point: degenerate cube, all keys equal, self exclusion
+    same = st.copy()
+    same["x"], same["y"], same["z"] = 1.5, 1.5, 1.5   # max == min: scale is inf, (x-min)*scale is NaN -> 0
+    with _ctx(gcs, same) as ctx:
+        ctx.run_stages(_params(gcs), gcs.STAGE_BOUNDS, gcs.STAGE_WALK)
+        assert np.all(ctx.read(gcs.BUF_KEYS) == 0)
+        assert np.all(ctx.read(gcs.BUF_ACCEL)[:, :3] == 0)
+        assert ctx.device_status() == 0
+    # two particles
+    with _ctx(gcs, st[:2]) as ctx:
+        p = _params(gcs)
+        ctx.run_stages(p, gcs.STAGE_BOUNDS, gcs.STAGE_WALK)
+        sp = ctx.read(gcs.BUF_POS)
+        ex = oracle_mod.direct_fp64(sp, [0, 1], p.G, p.epsilon_sq)
+        _assert_acc(ctx.read(gcs.BUF_ACCEL)[:, :3], ex)
+    # a NaN position is reported through the device status word
+    bad = st.copy()
+    bad["x"][5] = np.nan
+    with _ctx(gcs, bad) as ctx:
+        ctx.run_stages(_params(gcs), gcs.STAGE_BOUNDS, gcs.STAGE_BOUNDS)
+        assert ctx.device_status(clear=True) & gcs.DEV_NONFINITE_POSITION
+        assert ctx.device_status() == 0
+
+
+def test_bad_arguments_are_rejected(gcs_mod, stars):
+    gcs = gcs_mod
+    with _ctx(gcs, stars) as ctx:
+        with pytest.raises(gcs.GcsError):
+            ctx.step(_params(gcs, leaf_size=0))
+        with pytest.raises(gcs.GcsError):
+            ctx.step(_params(gcs, leaf_size=33))
+        with pytest.raises(gcs.GcsError):
+            ctx.set_segments([len(stars) + 1])
+        with pytest.raises(gcs.GcsError):
+            ctx.set_segments([0, len(stars)])
+
+
+def test_dropin_cpp_api(gcs_mod, oracle_mod, stars):
+    """The reference's C++ entry points, called by their mangled names."""
+    gcs = gcs_mod
+    L = gcs.lib()
+    f = {}
+    for name, sym, res, args in [
+        ("init", "_Z9cuda_initi", C.c_bool, [C.c_int]),
+        ("cleanup", "_Z12cuda_cleanupv", None, []),
+        ("upload", "_Z25cuda_upload_initial_starsPK4Stari", None, [C.c_void_p, C.c_int]),
+        ("step", "_Z17cuda_physics_stepP4Starifffffb", C.c_float,
+         [C.c_void_p, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_bool]),
+        ("com", "_Z23cuda_get_center_of_massPfS_S_", None, [C.c_void_p] * 3),
+        ("alloc", "_Z26cuda_allocate_pinned_starsPP4Stari", None, [C.c_void_p, C.c_int]),
+        ("free", "_Z22cuda_free_pinned_starsP4Star", None, [C.c_void_p]),
+        ("reg", "_Z17cuda_register_vboj", None, [C.c_uint]),
+        ("unreg", "_Z19cuda_unregister_vbov", None, []),
+    ]:
+        fn = getattr(L, sym)
+        fn.restype, fn.argtypes = res, args
+        f[name] = fn
+    n = len(stars)
+    assert f["init"](n)
+    try:
+        f["upload"](stars.ctypes.data, n)
+        pinned = C.c_void_p()
+        f["alloc"](C.byref(pinned), n)
+        assert pinned.value
+        host = np.ctypeslib.as_array((C.c_byte * (32 * n)).from_address(pinned.value)).view(gcs.STAR_DTYPE)
+        pos, vel = gcs.pos_vel_from_stars(stars)
+        lo, hi = oracle_mod.bounds(pos)
+        dt = f["step"](pinned, n, 1.0, 10.0, 0.01, float(lo), float(hi), False)
+        assert dt == pytest.approx(0.01)
+        xr, vr, ar, nodes = oracle_mod.step(pos, vel, 1.0, 10.0, 1.0, 1, 0.01, bounds_lohi=(lo, hi))
+        sr = gcs.stars_from_pos_vel(xr, vr)
+        for k in ("x", "y", "z", "vx", "vy", "vz"):
+            np.testing.assert_allclose(host[k], sr[k], rtol=1e-6, atol=1e-6)
+        np.testing.assert_array_equal(host["mass"], sr["mass"])
+        cx, cy, cz = C.c_float(), C.c_float(), C.c_float()
+        f["com"](C.byref(cx), C.byref(cy), C.byref(cz))
+        np.testing.assert_allclose([cx.value, cy.value, cz.value],
+                                   [nodes["com_x"][0], nodes["com_y"][0], nodes["com_z"][0]], rtol=1e-5)
+        # interop: stepped stars go to the headless device buffer, host untouched
+        f["reg"](7)
+        before = host.copy()
+        f["step"](pinned, n, 1.0, 10.0, 0.01, float(lo), float(hi), True)
+        np.testing.assert_array_equal(host, before)
+        assert L.gcs_dropin_device_stars()
+        f["unreg"]()
+        f["free"](pinned)
+    finally:
+        f["cleanup"]()

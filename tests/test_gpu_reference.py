@@ -1,0 +1,103 @@
+"""GPU parity against the reference's own GPU engine (oracle/_ref/libref_cuda.so,
+compiled from the reference's cuda_engine.cu / karras_bvh.cuh / CUB) and
+against the golden vectors it produced (tests/golden/ref_gpu_*.npz).
+
+Same inputs, same G / eps^2 / dt / bounds / theta, leaf size 1, FP32 centre
+of mass (the reference's configuration).  Keys, permutation and topology
+must be identical; node masses, widths and boxes identical; accelerations
+within 1e-5 relative (see test_gpu_parity for the metric); the reference's
+aggregation has no memory fence, so its node values are compared after a
+fresh run, and positions/velocities after the step within FP32 rounding of
+the accelerations."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from conftest import rel_err, small_collision
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def _acc_ok(a, ref, p999=1e-5, pmax=1e-4):
+    scale = np.median(np.linalg.norm(ref, axis=1))
+    e = rel_err(a, ref, floor=1e-3 * scale)
+    assert np.percentile(e, 99.9) <= p999, np.percentile(e, 99.9)
+    assert e.max() <= pmax, e.max()
+
+
+def _engine_run(gcs, stars, G, eps2, theta, dt, lo, hi, leaf=1):
+    n = len(stars)
+    with gcs.Context(n) as ctx:
+        ctx.upload(stars)
+        p = gcs.reference_params(G=G, epsilon_sq=eps2, theta=theta, dt=dt, global_min=lo, global_max=hi,
+                                 leaf_size=leaf, bounds_mode=gcs.BOUNDS_CALLER, com_fp64=0)
+        ctx.run_stages(p, gcs.STAGE_BOUNDS, gcs.STAGE_WALK)
+        out = dict(keys=ctx.read(gcs.BUF_KEYS), perm=ctx.read(gcs.BUF_INDEX), nodes=ctx.read(gcs.BUF_NODES),
+                   build=ctx.read(gcs.BUF_BUILD), leaf_parent=ctx.read(gcs.BUF_LEAF_PARENT),
+                   acc=ctx.read(gcs.BUF_ACCEL), pos=ctx.read(gcs.BUF_POS))
+        ctx.run_stages(p, gcs.STAGE_INTEGRATE, gcs.STAGE_INTEGRATE)
+        out["stars"] = ctx.download()
+        assert ctx.device_status() == 0
+    return out
+
+
+def _compare(gcs, mine, keys, perm, nodes, build, accels, soa, rgbt, n):
+    np.testing.assert_array_equal(mine["keys"], keys)
+    np.testing.assert_array_equal(mine["perm"].astype(np.int32), perm)
+    mn = mine["nodes"]
+    np.testing.assert_array_equal(mn["child_left"], nodes["child_left"][: n - 1])
+    np.testing.assert_array_equal(mn["child_right"], nodes["child_right"][: n - 1])
+    np.testing.assert_array_equal(mine["build"]["parent"], build["parent"][: n - 1])
+    np.testing.assert_array_equal(mine["leaf_parent"], build["parent"][n - 1:])
+    np.testing.assert_array_equal(mn["mass"], nodes["mass"][: n - 1])
+    np.testing.assert_array_equal(mn["width"], nodes["width"][: n - 1])
+    mb = mine["build"]
+    np.testing.assert_array_equal(np.stack([mb["min_x"], mb["min_y"], mb["min_z"]], 1), build["min"][: n - 1])
+    np.testing.assert_array_equal(np.stack([mb["max_x"], mb["max_y"], mb["max_z"]], 1), build["max"][: n - 1])
+    for k, a in enumerate(("com_x", "com_y", "com_z")):
+        r = nodes[a][: n - 1]
+        np.testing.assert_allclose(mn[a], r, rtol=1e-6, atol=1e-6 * np.abs(r).max())
+    _acc_ok(mine["acc"][:, :3], accels)
+    s = mine["stars"]
+    for k, f in enumerate(("x", "y", "z", "vx", "vy", "vz")):
+        np.testing.assert_allclose(s[f], soa[k], rtol=1e-5, atol=1e-5 * np.abs(soa[k]).max())
+    np.testing.assert_array_equal(s["mass"], soa[6])
+    np.testing.assert_array_equal(s["type"], rgbt[3])
+    # colours: identical wherever the velocities are (they depend on them)
+    same_v = (s["vx"] == soa[3]) & (s["vy"] == soa[4]) & (s["vz"] == soa[5])
+    for k, f in enumerate(("r", "g", "b")):
+        np.testing.assert_array_equal(s[f][same_v], rgbt[k][same_v])
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "ref_gpu_*.npz"))))
+def test_engine_matches_reference_gpu_golden(gcs_mod, path):
+    g = np.load(path)
+    st = g["stars"]
+    G, eps2, theta, dt, lo, hi = [float(x) for x in g["params"]]
+    mine = _engine_run(gcs_mod, st, G, eps2, theta, dt, lo, hi)
+    _compare(gcs_mod, mine, g["keys"], g["perm"], g["nodes"], g["build"], g["accels"], g["soa"], g["rgbt"], len(st))
+
+
+@pytest.mark.parametrize("theta,eps2", [(1.0, 10.0), (0.5, 0.0025)])
+def test_engine_matches_live_reference(gcs_mod, oracle_mod, theta, eps2):
+    ref_lib = oracle_mod.ref_lib("ref_cuda")
+    if ref_lib is None:
+        pytest.skip("oracle/_ref/libref_cuda.so not built (needs the reference sources)")
+    gcs = gcs_mod
+    st = gcs.collision_equal(*gcs.SMALL_COUNTS, seed=4)
+    n = len(st)
+    pos, _ = gcs.pos_vel_from_stars(st)
+    lo, hi = oracle_mod.bounds(pos)
+    ref = oracle_mod.RefCuda(n)
+    try:
+        ref.set_theta(theta)
+        ref.upload(st)
+        ref.step_device(1.0, eps2, 0.005, lo, hi)
+        rec = [ref.read(k) for k in range(7)]
+    finally:
+        ref.close()
+    mine = _engine_run(gcs, st, 1.0, eps2, theta, 0.005, lo, hi)
+    _compare(gcs, mine, *rec, n)
