@@ -53,6 +53,16 @@ __device__ __forceinline__ float softened_d2(float dx, float dy, float dz, float
     return __fadd_rn(__fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx))), eps2);
 }
 
+// ---- 1/sqrt of a softened distance ------------------------------------------
+// The reference's rsqrtf (cuda_engine.cu:135,144) is the hardware reciprocal
+// square root; for normal inputs the flush-to-zero form below returns the
+// same value without the subnormal-input fix-up, and d2 >= eps^2 > 0 here.
+__device__ __forceinline__ float rsqrt_approx(float x) {
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 // ---- opening criterion (cuda_engine.cu:143 with theta) ---------------------
 // A node is used as a monopole iff width^2 < theta^2 * d2 (d2 softened).
 // width^2 is formed once per node when it is staged.

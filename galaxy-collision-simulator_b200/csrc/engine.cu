@@ -55,6 +55,8 @@ struct gcs_ctx {
     int64_t targets_cap = 0;
     double* direct_out = nullptr;
     unsigned long long* counts = nullptr;  // walk interaction counters (count mode)
+    int2* walk_stack = nullptr;            // per-warp global bottoms of the walk stacks
+    size_t walk_stack_entries = 0;
     bool count_walk = false;
 
     std::string last_error;
@@ -63,9 +65,9 @@ struct gcs_ctx {
 namespace {
 
 constexpr int kChunkSize = 8192;
-// StepScratch rounded up to 256 bytes; the bounds and look-back regions follow.
-constexpr size_t kScratchHeader = (sizeof(StepScratch) + 255) & ~(size_t)255;
-static_assert(kScratchHeader >= sizeof(StepScratch), "scratch header must hold StepScratch");
+constexpr int kCountWords = 6;  // counting-walk outputs (gcs_count_interactions)
+
+size_t round256(size_t b) { return (b + 255) & ~(size_t)255; }
 
 void set_error(gcs_ctx* c, const char* what, cudaError_t e) {
     char buf[256];
@@ -103,19 +105,20 @@ Layout layout_of(const gcs_ctx* c) {
 
 int seg_passes(int nseg) { return nseg <= 1 ? 0 : (nseg <= 256 ? 1 : 2); }
 
-StepScratch* scratch_header(gcs_ctx* c) { return reinterpret_cast<StepScratch*>(c->scratch); }
-uint32_t* scratch_bounds(gcs_ctx* c) {
-    return reinterpret_cast<uint32_t*>(c->scratch + kScratchHeader);
+// Byte offsets of the scratch regions for n particles in nseg segments.
+ScratchLayout scratch_layout(int32_t max_segments, int64_t n, int nseg) {
+    ScratchLayout s;
+    s.hist = 0;
+    s.walk_q = round256(sizeof(uint32_t) * kMaxPasses * kRadix);
+    s.bounds = s.walk_q + 256;
+    s.tiles = s.bounds + round256(sizeof(uint32_t) * 2 * (size_t)max_segments);
+    s.lookback = s.tiles + 256;
+    s.end = s.lookback + sizeof(uint32_t) * sort_lookback_words(n, kKeyPasses + seg_passes(nseg));
+    return s;
 }
-uint32_t* scratch_lookback(gcs_ctx* c) {
-    size_t b = kScratchHeader + sizeof(uint32_t) * 2 * (size_t)c->max_segments;
-    b = (b + 255) & ~(size_t)255;
-    return reinterpret_cast<uint32_t*>(c->scratch + b);
-}
-size_t scratch_bytes_for(const gcs_ctx* c, int64_t n) {
-    size_t b = kScratchHeader + sizeof(uint32_t) * 2 * (size_t)c->max_segments;
-    b = (b + 255) & ~(size_t)255;
-    return b + sizeof(uint32_t) * sort_lookback_words(n, kKeyPasses + seg_passes(c->nseg));
+template <typename T>
+T* scratch_at(gcs_ctx* c, size_t off) {
+    return reinterpret_cast<T*>(c->scratch + off);
 }
 
 template <typename T>
@@ -133,7 +136,8 @@ void free_all(gcs_ctx* c) {
     void* ptrs[] = {c->pos[0], c->pos[1], c->vel[0], c->vel[1], c->acc, c->keys[0], c->keys[1],
                     c->idx[0], c->idx[1], c->tr, c->bd, c->com64, c->leaf_parent, c->seg_off,
                     c->seg_id, c->groups, c->chunks, c->seg_bounds, c->staging, c->pb_staging,
-                    c->scratch, c->status, c->diag, c->targets, c->direct_out, c->counts};
+                    c->scratch, c->status, c->diag, c->targets, c->direct_out, c->counts,
+                    c->walk_stack};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }
@@ -169,28 +173,30 @@ static int run_stage(gcs_ctx* c, const gcs_params* p, int stage) {
     cudaStream_t st = c->stream;
     const Layout L = layout_of(c);
     const int passes = kKeyPasses + seg_passes(c->nseg);
-    StepScratch* ss = scratch_header(c);
+    const ScratchLayout sl = scratch_layout(c->max_segments, c->n, c->nseg);
+    uint32_t* hist = scratch_at<uint32_t>(c, sl.hist);
     switch (stage) {
         case GCS_STAGE_BOUNDS: {
-            GCS_CUDA(c, cudaMemsetAsync(c->scratch, 0, scratch_bytes_for(c, c->n), st));
             if (p->bounds_mode == GCS_BOUNDS_DEVICE) {
-                launch_bounds(L, c->pos[c->cur], c->chunks, c->n_chunks, scratch_bounds(c),
-                              c->status, st);
-                launch_bounds_decode(scratch_bounds(c), c->seg_bounds, c->nseg, st);
+                uint32_t* enc = scratch_at<uint32_t>(c, sl.bounds);
+                GCS_CUDA(c, cudaMemsetAsync(enc, 0, sizeof(uint32_t) * 2 * (size_t)c->nseg, st));
+                launch_bounds(L, c->pos[c->cur], c->chunks, c->n_chunks, enc, c->status, st);
+                launch_bounds_decode(enc, c->seg_bounds, c->nseg, st);
             }
             return check_launch(c, "bounds");
         }
         case GCS_STAGE_ENCODE:
+            GCS_CUDA(c, cudaMemsetAsync(hist, 0, sizeof(uint32_t) * kRadix * (size_t)passes, st));
             launch_encode(L, c->pos[c->cur], p->bounds_mode, p->global_min, p->global_max,
-                          c->seg_bounds, c->keys[0], c->idx[0], &ss->hist[0][0],
-                          seg_passes(c->nseg), st);
+                          c->seg_bounds, c->keys[0], c->idx[0], hist, seg_passes(c->nseg), st);
             return check_launch(c, "encode");
         case GCS_STAGE_SORT: {
+            GCS_CUDA(c, cudaMemsetAsync(c->scratch + sl.tiles, 0, sl.end - sl.tiles, st));
             for (int pass = 0; pass < passes; ++pass) {
                 const int in = pass & 1;
                 launch_sort_pass(L, pass, c->keys[in], c->idx[in], c->keys[in ^ 1], c->idx[in ^ 1],
-                                 &ss->hist[0][0], ss->tile_counter, scratch_lookback(c), c->status,
-                                 st);
+                                 hist, scratch_at<uint32_t>(c, sl.tiles),
+                                 scratch_at<uint32_t>(c, sl.lookback), c->status, st);
             }
             c->sorted_buf = passes & 1;
             return check_launch(c, "sort");
@@ -216,8 +222,8 @@ static int run_stage(gcs_ctx* c, const gcs_params* p, int stage) {
             wp.batch = p->walk_batch > 0 ? p->walk_batch : default_walk_batch();
             wp.with_potential = p->with_potential ? 1 : 0;
             launch_walk(L, wp, c->pos[c->cur], c->tr, c->groups, c->n_groups, c->acc,
-                        &ss->walk_counter, c->status, p->walk_blocks_per_sm, c->sm_count,
-                        c->count_walk ? c->counts : nullptr, st);
+                        scratch_at<uint32_t>(c, sl.walk_q), c->status, p->walk_blocks_per_sm, c->sm_count,
+                        c->count_walk ? c->counts : nullptr, c->walk_stack, c->walk_stack_entries, st);
             return check_launch(c, "walk");
         }
         case GCS_STAGE_INTEGRATE:
@@ -340,11 +346,17 @@ int gcs_create(gcs_ctx** out, int64_t capacity, int32_t max_segments, int32_t de
     if (!rc) rc |= dalloc(c, &c->pb_staging, N);
     if (!rc) rc |= dalloc(c, &c->status, 1);
     if (!rc) rc |= dalloc(c, &c->diag, 8);
-    if (!rc) rc |= dalloc(c, &c->counts, 2);
+    if (!rc) rc |= dalloc(c, &c->counts, kCountWords);
     if (!rc) {
-        c->nseg = max_segments;  // worst case for the scratch size
-        c->scratch_cap = scratch_bytes_for(c, capacity) + 256;
-        c->nseg = 0;
+        // enough per-warp stack regions for the largest persistent walk grid
+        const int64_t gb = std::max(walk_grid_blocks((int)max_groups, 0, c->sm_count, 0),
+                                    walk_grid_blocks((int)max_groups, 0, c->sm_count, 1));
+        c->walk_stack_entries = walk_stack_entries(gb);
+        rc |= dalloc(c, &c->walk_stack, c->walk_stack_entries);
+    }
+    if (!rc) {
+        // worst case: every particle, the most segment-id sort passes
+        c->scratch_cap = scratch_layout(max_segments, capacity, max_segments).end;
         rc |= dalloc(c, &c->scratch, c->scratch_cap);
     }
     if (rc) {
@@ -352,6 +364,7 @@ int gcs_create(gcs_ctx** out, int64_t capacity, int32_t max_segments, int32_t de
         delete c;
         return GCS_ERR_NOMEM;
     }
+    cudaMemset(c->scratch, 0, c->scratch_cap);  // the walk queue starts (and stays) at zero
     cudaMemset(c->status, 0, sizeof(uint32_t));
     cudaMemset(c->acc, 0, sizeof(float4) * N);
     int64_t cnt = capacity;
@@ -577,15 +590,16 @@ int gcs_diagnostics(gcs_ctx* c, int32_t segment, double out[6]) {
     return GCS_OK;
 }
 
-int gcs_count_interactions(gcs_ctx* c, const gcs_params* p, uint64_t out[2]) {
+int gcs_count_interactions(gcs_ctx* c, const gcs_params* p, uint64_t out[6]) {
     if (!c || !p || !out) return GCS_ERR_ARG;
     cudaSetDevice(c->device);
-    GCS_CUDA(c, cudaMemsetAsync(c->counts, 0, 2 * sizeof(unsigned long long), c->stream));
+    GCS_CUDA(c, cudaMemsetAsync(c->counts, 0, kCountWords * sizeof(unsigned long long), c->stream));
     c->count_walk = true;
     const int rc = run_stages(c, p, GCS_STAGE_BOUNDS, GCS_STAGE_WALK);
     c->count_walk = false;
     if (rc) return rc;
-    GCS_CUDA(c, cudaMemcpyAsync(out, c->counts, 2 * sizeof(uint64_t), cudaMemcpyDeviceToHost, c->stream));
+    GCS_CUDA(c, cudaMemcpyAsync(out, c->counts, kCountWords * sizeof(uint64_t), cudaMemcpyDeviceToHost,
+                                c->stream));
     GCS_CUDA(c, cudaStreamSynchronize(c->stream));
     return GCS_OK;
 }

@@ -54,14 +54,15 @@ struct Layout {
     const int32_t* seg_id;   // device [n]
 };
 
-// Scratch zeroed at the start of each step (one memset).
-struct StepScratch {
-    uint32_t hist[kMaxPasses][kRadix];    // global digit histograms
-    uint32_t tile_counter[kMaxPasses];    // onesweep tile ticket per pass
-    uint32_t walk_counter;                // walk work-queue head
-    uint32_t pad[5];
-    // followed by: bounds u32[2*S] (ordered-float max of -min / max),
-    //              look-back u32[passes][tiles][256]
+// Per-step scratch, one device allocation.  Each stage zeroes only the
+// region it accumulates into, so any stage can be run on its own:
+//   hist      u32[kMaxPasses][256]  radix digit histograms   (zeroed by encode)
+//   walk_q    u32[2]                walk work queue          (self-resetting)
+//   bounds    u32[2 * max_segments] ordered min/max          (zeroed by bounds)
+//   tiles     u32[kMaxPasses]       onesweep tile tickets    (zeroed by sort,
+//   lookback  u32[passes][tiles][256] decoupled look-back      with lookback)
+struct ScratchLayout {
+    size_t hist, walk_q, bounds, tiles, lookback, end;
 };
 
 // ---- launchers (one per stage; all asynchronous on `st`) ----------------
@@ -97,11 +98,20 @@ struct WalkParams {
     int32_t batch;
     int32_t with_potential;
 };
+// Global-memory stack entries (int2) per walk warp: the shared-memory stack
+// spills its bottom here.  A round adds at most `batch` entries per tree
+// level, so 4096 covers batch 32 on trees 128 levels deep.
+constexpr int kWalkGlobalStack = 4096;
 void launch_walk(const Layout& L, const WalkParams& wp, const float4* pos,
                  const BvhNodeTraverse* tr, const WalkGroup* groups, int n_groups,
-                 float4* acc, uint32_t* work_counter, uint32_t* status, int blocks_per_sm,
-                 int sm_count, unsigned long long* counts, cudaStream_t st);
+                 float4* acc, uint32_t* queue, uint32_t* status, int blocks_per_sm,
+                 int sm_count, unsigned long long* counts, int2* gstack, size_t gstack_entries,
+                 cudaStream_t st);
 int walk_max_blocks_per_sm(int batch, int with_potential);
+// Persistent walk grid (blocks) for n_groups groups, and the global stack
+// entries that grid needs.
+int64_t walk_grid_blocks(int n_groups, int blocks_per_sm, int sm_count, int with_potential);
+size_t walk_stack_entries(int64_t grid_blocks);
 
 void launch_integrate(float4* pos, float4* vel, const float4* acc, float dt, int recolor,
                       int64_t n, cudaStream_t st);

@@ -70,7 +70,10 @@ __global__ void build_kernel(Layout L, const uint64_t* __restrict__ keys,
         } while (step > 1);
         const int split = i + s_ * d + (d > 0 ? 0 : -1);
         const int lo = min(i, j), hi = max(i, j);
-        if (split < lo || split + 1 > hi) atomicOr(status, GCS_DEV_BUILD_RANGE);
+        if (split < lo || split + 1 > hi) {  // cannot happen for sorted keys; never write out of range
+            atomicOr(status, GCS_DEV_BUILD_RANGE);
+            continue;
+        }
         const int node = node_base + i;
         const int cl = (lo == split) ? leaf_base + split : node_base + split;
         const int cr = (hi == split + 1) ? leaf_base + split + 1 : node_base + split + 1;
@@ -146,6 +149,10 @@ __global__ void aggregate_kernel(Layout L, const float4* __restrict__ pos,
             __threadfence();
             const int cl = __ldcg(&tr[node].child_left);
             const int cr = __ldcg(&tr[node].child_right);
+            if (cl < 0 || cr < 0 || cl >= L.n_internal + L.n || cr >= L.n_internal + L.n) {
+                atomicOr(status, GCS_DEV_TREE_MALFORMED);
+                break;
+            }
             const ChildData A = load_child(cl, L.n_internal, pos, tr, bd, com64, fp64);
             const ChildData B = load_child(cr, L.n_internal, pos, tr, bd, com64, fp64);
             const float3 lo = make_float3(fminf(A.lo.x, B.lo.x), fminf(A.lo.y, B.lo.y),

@@ -279,10 +279,13 @@ class Context:
         self.check(self.L.gcs_diagnostics(self._h, segment, out))
         return np.array(out[:])
 
-    def count_interactions(self, p: Params) -> tuple[int, int]:
-        out = (C.c_uint64 * 2)()
+    def count_interactions(self, p: Params, warp_evals: bool = False):
+        """(monopole terms, particle terms)[, warp node evals, warp source evals,
+        pop rounds, single-node rounds]."""
+        out = (C.c_uint64 * 6)()
         self.check(self.L.gcs_count_interactions(self._h, C.byref(p), out))
-        return int(out[0]), int(out[1])
+        r = tuple(int(x) for x in out)
+        return r if warp_evals else r[:2]
 
     def direct_fp64(self, p: Params, targets, segment: int = 0) -> np.ndarray:
         t = np.ascontiguousarray(targets, dtype=np.int64)
