@@ -65,7 +65,7 @@ struct gcs_ctx {
 namespace {
 
 constexpr int kChunkSize = 8192;
-constexpr int kCountWords = 6;  // counting-walk outputs (gcs_count_interactions)
+constexpr int kCountWords = 8;  // counting-walk outputs (gcs_count_interactions)
 
 size_t round256(size_t b) { return (b + 255) & ~(size_t)255; }
 
@@ -590,7 +590,7 @@ int gcs_diagnostics(gcs_ctx* c, int32_t segment, double out[6]) {
     return GCS_OK;
 }
 
-int gcs_count_interactions(gcs_ctx* c, const gcs_params* p, uint64_t out[6]) {
+int gcs_count_interactions(gcs_ctx* c, const gcs_params* p, uint64_t out[8]) {
     if (!c || !p || !out) return GCS_ERR_ARG;
     cudaSetDevice(c->device);
     GCS_CUDA(c, cudaMemsetAsync(c->counts, 0, kCountWords * sizeof(unsigned long long), c->stream));

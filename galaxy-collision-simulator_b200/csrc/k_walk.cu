@@ -65,13 +65,21 @@ constexpr uint32_t kFull = 0xFFFFFFFFu;
 constexpr int kBucketTag = 1 << 30;
 constexpr int kSkipTag = 0x7FFFFFFF;
 
+// Classes of a batch node against the group's bounding box.
+constexpr int kClassNone = 0;   // lane holds no node
+constexpr int kClassTake = 1;   // every lane of the group accepts it
+constexpr int kClassOpen = 2;   // every lane of the group opens it
+constexpr int kClassMixed = 3;  // lanes decide one by one
+constexpr float kBoxLo = 1.0f - 1.0f / 65536.0f;
+constexpr float kBoxHi = 1.0f + 1.0f / 65536.0f;
+
 struct WarpSmem {
     int2 stk[kStackCap];          // node, lane mask
-    float4 nc[kMaxBatch];         // com x, y, z, G*mass
+    float4 nc[kMaxBatch];         // com x, y, z, G*mass (compacted: take, then mixed)
+    uint2 nw[kMaxBatch];          // bits of width^2, lane mask
+    uint32_t nopen[kMaxBatch];    // opening lanes of each mixed node
     float4 src[kSrcCap];          // x, y, z, G*mass
     int2 srcm[kSrcCap];           // particle, lane mask
-    uint32_t nw2[kMaxBatch];      // bits of width^2 ... and the node's lane mask:
-    uint32_t nmask[kMaxBatch];
 };
 
 struct Accum {
@@ -79,6 +87,7 @@ struct Accum {
     uint32_t n_mono, n_part;  // interaction counts (count mode only)
     uint32_t w_node, w_src;   // warp-wide node / source evaluations (count mode only)
     uint32_t rounds, spills;  // pop rounds, stack spills to global memory
+    uint32_t all_open, all_take;  // node evaluations opened / accepted by every active lane
 };
 
 // Sum the listed particle sources into every lane whose bit is in the
@@ -156,11 +165,23 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
         const int t = grp.start + lane;
         const float4 p = valid ? __ldg(pos + t) : make_float4(0.f, 0.f, 0.f, 0.f);
         const uint32_t live = __ballot_sync(kFull, valid);
+        // bounding box of the group's targets
+        float3 box_lo = valid ? make_float3(p.x, p.y, p.z) : make_float3(INFINITY, INFINITY, INFINITY);
+        float3 box_hi = valid ? make_float3(p.x, p.y, p.z) : make_float3(-INFINITY, -INFINITY, -INFINITY);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            box_lo.x = fminf(box_lo.x, __shfl_xor_sync(kFull, box_lo.x, o));
+            box_lo.y = fminf(box_lo.y, __shfl_xor_sync(kFull, box_lo.y, o));
+            box_lo.z = fminf(box_lo.z, __shfl_xor_sync(kFull, box_lo.z, o));
+            box_hi.x = fmaxf(box_hi.x, __shfl_xor_sync(kFull, box_hi.x, o));
+            box_hi.y = fmaxf(box_hi.y, __shfl_xor_sync(kFull, box_hi.y, o));
+            box_hi.z = fmaxf(box_hi.z, __shfl_xor_sync(kFull, box_hi.z, o));
+        }
         const int s = grp.seg;
         const int off = (int)__ldg(L.seg_off + s);
         const int seg_n = (int)__ldg(L.seg_off + s + 1) - off;
         const int seg_end = off + seg_n;
-        Accum A = {0.f, 0.f, 0.f, 0.f, 0u, 0u, 0u, 0u, 0u, 0u};
+        Accum A = {0.f, 0.f, 0.f, 0.f, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
         int nsrc = 0;
 
         if (seg_n >= 2) {
@@ -189,8 +210,12 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                     break;
                 }
                 top -= b;
-                // 1. fetch and digest node `lane` of the batch
+                // 1. fetch, digest and classify node `lane` of the batch
                 int code_a = 0, code_b = kSkipTag;
+                int cls = kClassNone;
+                float w2 = 0.0f;
+                float4 com = make_float4(0.f, 0.f, 0.f, 0.f);
+                uint32_t my_mask = 0u;
                 if (lane < b) {
                     const int2 e = W.stk[top + lane];
                     const float4* np = reinterpret_cast<const float4*>(tr + e.x);
@@ -213,27 +238,76 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                             atomicOr(status, GCS_DEV_BUILD_RANGE);
                         }
                     }
-                    W.nc[lane] = a;
-                    W.nw2[lane] = __float_as_uint(__fmul_rn(c.x, c.x));
-                    W.nmask[lane] = (uint32_t)e.y;
+                    w2 = __fmul_rn(c.x, c.x);
+                    com = a;
+                    my_mask = (uint32_t)e.y;
+                    // Classify against the group's box.  With a 2^-16 relative
+                    // margin (far above the few-ulp rounding of any lane's own
+                    // d2 or of these sums) "take" guarantees every lane in the
+                    // box accepts, "open" that every lane opens.
+                    float s2min = 0.0f, s2max = 0.0f;
+                    {
+                        const float dl[3] = {box_lo.x - a.x, box_lo.y - a.y, box_lo.z - a.z};
+                        const float dh[3] = {a.x - box_hi.x, a.y - box_hi.y, a.z - box_hi.z};
+#pragma unroll
+                        for (int ax = 0; ax < 3; ++ax) {
+                            const float near = fmaxf(fmaxf(dl[ax], dh[ax]), 0.0f);
+                            const float far = fmaxf(fabsf(dl[ax]), fabsf(dh[ax]));
+                            s2min = fmaf(near, near, s2min);
+                            s2max = fmaf(far, far, s2max);
+                        }
+                    }
+                    if (w2 < theta2 * (s2min + eps2) * kBoxLo) cls = kClassTake;
+                    else if (w2 >= theta2 * (s2max + eps2) * kBoxHi) cls = kClassOpen;
+                    else cls = kClassMixed;
+                }
+                // compact: accepted-by-all nodes first, then mixed ones
+                const uint32_t bt = __ballot_sync(kFull, cls == kClassTake);
+                const uint32_t bm = __ballot_sync(kFull, cls == kClassMixed);
+                const int n_take = __popc(bt), n_mixed = __popc(bm);
+                const uint32_t lt = lane_bit - 1u;
+                const int slot = cls == kClassTake ? __popc(bt & lt)
+                                                   : (cls == kClassMixed ? n_take + __popc(bm & lt) : -1);
+                if (slot >= 0) {
+                    W.nc[slot] = com;
+                    W.nw[slot] = make_uint2(__float_as_uint(w2), my_mask);
                 }
                 __syncwarp();
                 if (kCount) {
                     A.w_node += (uint32_t)b;
                     A.rounds += 1u;
+                    A.all_open += (uint32_t)(b - n_take - n_mixed);
+                    A.all_take += (uint32_t)n_take;
                 }
-                // 2. branch-free evaluation of the batch
-                uint32_t my_open = 0u;
+                // 2a. nodes every lane accepts: monopole terms only
 #pragma unroll 2
-                for (int k = 0; k < b; ++k) {
+                for (int k = 0; k < n_take; ++k) {
                     const float4 a = W.nc[k];
-                    const float w2 = __uint_as_float(W.nw2[k]);
-                    const bool active = (W.nmask[k] & lane_bit) != 0u;
+                    const bool active = (W.nw[k].y & lane_bit) != 0u;
                     const float dx = __fsub_rn(a.x, p.x);
                     const float dy = __fsub_rn(a.y, p.y);
                     const float dz = __fsub_rn(a.z, p.z);
                     const float d2 = softened_d2(dx, dy, dz, eps2);
-                    const bool take = accept_monopole(w2, d2, theta2);
+                    const float inv = rsqrt_approx(d2);
+                    const float inv3 = __fmul_rn(__fmul_rn(inv, inv), inv);
+                    const float f = active ? __fmul_rn(a.w, inv3) : 0.0f;
+                    A.ax = __fmaf_rn(dx, f, A.ax);
+                    A.ay = __fmaf_rn(dy, f, A.ay);
+                    A.az = __fmaf_rn(dz, f, A.az);
+                    if (kPot) A.pot = active ? __fmaf_rn(-a.w, inv, A.pot) : A.pot;
+                    if (kCount) A.n_mono += active ? 1u : 0u;
+                }
+                // 2b. mixed nodes: each lane's own test; lane 0 records the
+                // ballot of opening lanes for the node's owner
+                for (int k = n_take; k < n_take + n_mixed; ++k) {
+                    const float4 a = W.nc[k];
+                    const uint2 wm = W.nw[k];
+                    const bool active = (wm.y & lane_bit) != 0u;
+                    const float dx = __fsub_rn(a.x, p.x);
+                    const float dy = __fsub_rn(a.y, p.y);
+                    const float dz = __fsub_rn(a.z, p.z);
+                    const float d2 = softened_d2(dx, dy, dz, eps2);
+                    const bool take = accept_monopole(__uint_as_float(wm.x), d2, theta2);
                     const bool mono = active && take;
                     const float inv = rsqrt_approx(d2);
                     const float inv3 = __fmul_rn(__fmul_rn(inv, inv), inv);
@@ -244,8 +318,12 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                     if (kPot) A.pot = mono ? __fmaf_rn(-a.w, inv, A.pot) : A.pot;
                     if (kCount) A.n_mono += mono ? 1u : 0u;
                     const uint32_t om = __ballot_sync(kFull, active && !take);
-                    my_open = lane == k ? om : my_open;
+                    if (lane == 0) W.nopen[k] = om;
                 }
+                __syncwarp();
+                uint32_t my_open = 0u;
+                if (cls == kClassOpen) my_open = my_mask;
+                else if (cls == kClassMixed) my_open = W.nopen[slot];
                 // 3. parallel push / append for the opened nodes
                 int n_push = 0, n_src = 0;
                 if (my_open != 0u && code_b != kSkipTag) {
@@ -334,6 +412,8 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                 atomicAdd(counts + 3, (unsigned long long)A.w_src);
                 atomicAdd(counts + 4, (unsigned long long)A.rounds);
                 atomicAdd(counts + 5, (unsigned long long)A.spills);
+                atomicAdd(counts + 6, (unsigned long long)A.all_open);
+                atomicAdd(counts + 7, (unsigned long long)A.all_take);
             }
         }
         __syncwarp();

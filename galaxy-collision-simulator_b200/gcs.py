@@ -281,8 +281,8 @@ class Context:
 
     def count_interactions(self, p: Params, warp_evals: bool = False):
         """(monopole terms, particle terms)[, warp node evals, warp source evals,
-        pop rounds, single-node rounds]."""
-        out = (C.c_uint64 * 6)()
+        pop rounds, stack spills, evals opened by all lanes, evals accepted by all]."""
+        out = (C.c_uint64 * 8)()
         self.check(self.L.gcs_count_interactions(self._h, C.byref(p), out))
         r = tuple(int(x) for x in out)
         return r if warp_evals else r[:2]

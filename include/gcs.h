@@ -220,9 +220,10 @@ int gcs_diagnostics(gcs_ctx* ctx, int32_t segment, double out[6]);
  * summed over all targets (the unit of interactions/s; 20 FP32 flops each),
  * then the warp-wide {node evaluations, particle-source evaluations} (each
  * serves up to 32 targets; terms / (32 * evaluations) is the lane
- * utilisation of the group walk), then {stack pop rounds, rounds limited to
- * a single node by the stack bound}. */
-int gcs_count_interactions(gcs_ctx* ctx, const gcs_params* p, uint64_t out[6]);
+ * utilisation of the group walk), then {stack pop rounds, stack spills to
+ * global memory}, then {node evaluations opened by every active lane, node
+ * evaluations accepted by every active lane}. */
+int gcs_count_interactions(gcs_ctx* ctx, const gcs_params* p, uint64_t out[8]);
 /* FP64 direct-sum accelerations (excluding only i == j) at `n_targets`
  * sorted positions `targets` of one segment; result as double[3*n_targets].
  * Reads the current positions; eps^2 and G from p. */
