@@ -56,8 +56,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["gcs", "reference"], default="gcs")
     ap.add_argument("--n", type=int, default=N_DEFAULT, help="particles (default: the 1M config)")
-    ap.add_argument("--leaf", type=int, default=0, help="leaf size (0: tuned default)")
-    ap.add_argument("--batch", type=int, default=0, help="walk nodes per pop (0: tuned default)")
+    ap.add_argument("--leaf", type=int, default=0, help="leaf size (0: autotuned, <= 32)")
+    ap.add_argument("--batch", type=int, default=0, help="walk nodes per pop (0: autotuned)")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")
@@ -271,11 +271,19 @@ def main():
 
     stars = gcs.collision_equal(*counts_for(args.n), seed=rank)
     n = len(stars)
-    leaf = args.leaf if args.leaf > 0 else 16
-    p = make_params(gcs, leaf, args.batch)
     stream = torch.cuda.current_stream()
     ctx = gcs.Context(n, device=local)
     ctx.set_stream(stream.cuda_stream)
+    ctx.upload(stars)
+    tuned = None
+    if args.leaf > 0 and args.batch > 0:
+        p = make_params(gcs, args.leaf, args.batch)
+    else:
+        # the recipe's "leaf <= 32": the autotuner picks leaf size, pop batch,
+        # group width and occupancy on the initial state (outside the timing)
+        p, tune_ms = ctx.autotune(make_params(gcs, args.leaf if args.leaf > 0 else 32, args.batch))
+        tuned = {"leaf_size": p.leaf_size, "walk_batch": p.walk_batch, "blocks_per_sm": p.walk_blocks_per_sm,
+                 "group_width": ctx.group_width, "walk_ms": tune_ms}
     ctx.upload(stars)
     n_mono, n_part = ctx.count_interactions(p)
     ctx.upload(stars)
@@ -353,8 +361,9 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded two-galaxy initial conditions, seed = rank)",
-            "config": {"workload": WORKLOAD, "particles": n, "leaf_size": leaf,
-                       "walk_batch": args.batch or 16, "com": "fp64 sums", "bounds": "device, per step",
+            "config": {"workload": WORKLOAD, "particles": n, "leaf_size": p.leaf_size,
+                       "walk_batch": p.walk_batch, "group_width": ctx.group_width, "autotuned": tuned,
+                       "com": "fp64 sums", "bounds": "device, per step",
                        "l2": "working set ~270 MB > 126 MB L2; no flush", "parallelism": "replicas x%d" % world},
             "e2e": e2e, "roofline": roofline, "clocks": clocks, "gpu_launches": launches_per_step * args.steps,
             "device_status": status}

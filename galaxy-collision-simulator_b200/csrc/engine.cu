@@ -57,6 +57,8 @@ struct gcs_ctx {
     unsigned long long* counts = nullptr;  // walk interaction counters (count mode)
     int2* walk_stack = nullptr;            // per-warp global bottoms of the walk stacks
     size_t walk_stack_entries = 0;
+    int32_t group_width = 32;              // targets per walk group (<= 32)
+    size_t groups_cap = 0;
     bool count_walk = false;
 
     std::string last_error;
@@ -66,6 +68,7 @@ namespace {
 
 constexpr int kChunkSize = 8192;
 constexpr int kCountWords = 8;  // counting-walk outputs (gcs_count_interactions)
+constexpr int kMinGroupWidth = 8;
 
 size_t round256(size_t b) { return (b + 255) & ~(size_t)255; }
 
@@ -162,7 +165,34 @@ int validate_params(gcs_ctx* c, const gcs_params* p) {
     return GCS_OK;
 }
 
-int default_walk_batch() { return 16; }
+int default_walk_batch() { return 32; }
+
+// Walk work units: runs of <= group_width consecutive particles that never
+// straddle a segment, so a segment's groups are the same alone or batched.
+int upload_groups(gcs_ctx* c) {
+    std::vector<WalkGroup> groups;
+    groups.reserve((size_t)(c->n / c->group_width + c->nseg + 1));
+    for (int s = 0; s < c->nseg; ++s) {
+        const int64_t a = c->h_seg_off[s], e = c->h_seg_off[s + 1];
+        for (int64_t g = a; g < e; g += c->group_width) {
+            WalkGroup w;
+            w.start = (int32_t)g;
+            w.count = (int32_t)std::min<int64_t>(c->group_width, e - g);
+            w.seg = s;
+            w.pad = 0;
+            groups.push_back(w);
+        }
+    }
+    if (groups.size() > c->groups_cap) {
+        c->last_error = "group table capacity exceeded";
+        return GCS_ERR_CAPACITY;
+    }
+    cudaSetDevice(c->device);
+    GCS_CUDA(c, cudaMemcpy(c->groups, groups.data(), sizeof(WalkGroup) * groups.size(),
+                           cudaMemcpyHostToDevice));
+    c->n_groups = (int)groups.size();
+    return GCS_OK;
+}
 
 }  // namespace
 
@@ -323,7 +353,9 @@ int gcs_create(gcs_ctx** out, int64_t capacity, int32_t max_segments, int32_t de
     c->capacity = capacity;
     c->max_segments = max_segments;
     const size_t N = (size_t)capacity;
-    const size_t max_groups = N / kGroupSize + (size_t)max_segments + 1;
+    // groups as narrow as kMinGroupWidth targets (the autotuner's smallest)
+    const size_t max_groups = N / kMinGroupWidth + (size_t)max_segments + 1;
+    c->groups_cap = max_groups;
     const size_t max_chunks = N / kChunkSize + (size_t)max_segments + 1;
     int rc = GCS_OK;
     for (int b = 0; b < 2 && !rc; ++b) {
@@ -415,19 +447,9 @@ int gcs_set_segments(gcs_ctx* c, int32_t num_segments, const int64_t* counts) {
     }
     const int64_t n = off[num_segments];
     std::vector<int32_t> sid((size_t)n);
-    std::vector<WalkGroup> groups;
     std::vector<Chunk> chunks;
-    groups.reserve((size_t)(n / kGroupSize + num_segments));
     for (int s = 0; s < num_segments; ++s) {
         for (int64_t i = off[s]; i < off[s + 1]; ++i) sid[(size_t)i] = s;
-        for (int64_t g = off[s]; g < off[s + 1]; g += kGroupSize) {
-            WalkGroup w;
-            w.start = (int32_t)g;
-            w.count = (int32_t)std::min<int64_t>(kGroupSize, off[s + 1] - g);
-            w.seg = s;
-            w.pad = 0;
-            groups.push_back(w);
-        }
         for (int64_t g = off[s]; g < off[s + 1]; g += kChunkSize) {
             Chunk ch;
             ch.start = (int32_t)g;
@@ -440,19 +462,24 @@ int gcs_set_segments(gcs_ctx* c, int32_t num_segments, const int64_t* counts) {
     cudaSetDevice(c->device);
     GCS_CUDA(c, cudaMemcpy(c->seg_off, off.data(), sizeof(int64_t) * off.size(), cudaMemcpyHostToDevice));
     GCS_CUDA(c, cudaMemcpy(c->seg_id, sid.data(), sizeof(int32_t) * sid.size(), cudaMemcpyHostToDevice));
-    GCS_CUDA(c, cudaMemcpy(c->groups, groups.data(), sizeof(WalkGroup) * groups.size(),
-                           cudaMemcpyHostToDevice));
     GCS_CUDA(c, cudaMemcpy(c->chunks, chunks.data(), sizeof(Chunk) * chunks.size(),
                            cudaMemcpyHostToDevice));
     c->h_seg_off = off;
     c->n = (int32_t)n;
     c->nseg = num_segments;
     c->n_internal = (int32_t)(n - num_segments);
-    c->n_groups = (int)groups.size();
     c->n_chunks = (int)chunks.size();
     c->cur = 0;
-    return GCS_OK;
+    return upload_groups(c);
 }
+
+int gcs_set_group_width(gcs_ctx* c, int32_t width) {
+    if (!c || width < kMinGroupWidth || width > kGroupSize) return GCS_ERR_ARG;
+    c->group_width = width;
+    return upload_groups(c);
+}
+
+int32_t gcs_group_width(const gcs_ctx* c) { return c ? c->group_width : 0; }
 
 int64_t gcs_num_particles(const gcs_ctx* c) { return c ? c->n : 0; }
 int32_t gcs_num_segments(const gcs_ctx* c) { return c ? c->nseg : 0; }
@@ -602,6 +629,63 @@ int gcs_count_interactions(gcs_ctx* c, const gcs_params* p, uint64_t out[8]) {
                                 c->stream));
     GCS_CUDA(c, cudaStreamSynchronize(c->stream));
     return GCS_OK;
+}
+
+int gcs_autotune(gcs_ctx* c, gcs_params* p, double* best_walk_ms) {
+    if (!c || !p) return GCS_ERR_ARG;
+    int rc = run_stages(c, p, GCS_STAGE_BOUNDS, GCS_STAGE_AGGREGATE);
+    if (rc) return rc;
+    cudaSetDevice(c->device);
+    cudaEvent_t e0, e1;
+    GCS_CUDA(c, cudaEventCreate(&e0));
+    GCS_CUDA(c, cudaEventCreate(&e1));
+    const int widths[] = {32, 16};
+    const int leaves[] = {1, 2, 4, 8, 16, 32};
+    const int batches[] = {16, 32};
+    const int occupancy[] = {0, 4};
+    gcs_params best = *p;
+    int best_width = c->group_width;
+    float best_ms = 3.0e38f;
+    for (int gw : widths) {
+        rc = gcs_set_group_width(c, gw);
+        if (rc) break;
+        for (int L : leaves) {
+            if (L > p->leaf_size) continue;
+            for (int b : batches) {
+                for (int occ : occupancy) {
+                    gcs_params q = *p;
+                    q.leaf_size = L;
+                    q.walk_batch = b;
+                    q.walk_blocks_per_sm = occ;
+                    if ((rc = run_stage(c, &q, GCS_STAGE_WALK))) break;  // warm
+                    cudaEventRecord(e0, c->stream);
+                    for (int r = 0; r < 2 && !rc; ++r) rc = run_stage(c, &q, GCS_STAGE_WALK);
+                    cudaEventRecord(e1, c->stream);
+                    if (rc) break;
+                    cudaEventSynchronize(e1);
+                    float ms = 0.0f;
+                    cudaEventElapsedTime(&ms, e0, e1);
+                    ms *= 0.5f;
+                    if (ms < best_ms) {
+                        best_ms = ms;
+                        best = q;
+                        best_width = gw;
+                    }
+                }
+                if (rc) break;
+            }
+            if (rc) break;
+        }
+        if (rc) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    rc = gcs_set_group_width(c, best_width);
+    if (rc) return rc;
+    *p = best;
+    if (best_walk_ms) *best_walk_ms = best_ms;
+    return gcs_synchronize(c);
 }
 
 int gcs_direct_accels_fp64(gcs_ctx* c, const gcs_params* p, int32_t segment,

@@ -27,6 +27,13 @@ namespace gcs {
 
 namespace {
 
+// Arrival counter increment with acquire-release semantics at GPU scope.
+__device__ __forceinline__ int arrive_acq_rel(int32_t* flag) {
+    int old;
+    asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], 1;" : "=r"(old) : "l"(flag) : "memory");
+    return old;
+}
+
 // Common prefix length of sorted keys i and j of one segment (local indices);
 // -1 when j falls outside the segment.
 __device__ __forceinline__ int lcp(int i, int j, int n, const uint64_t* __restrict__ k,
@@ -143,10 +150,11 @@ __global__ void aggregate_kernel(Layout L, const float4* __restrict__ pos,
                 atomicOr(status, GCS_DEV_TREE_MALFORMED);
                 break;
             }
-            __threadfence();
-            const int old = atomicAdd(&bd[node].flag, 1);
+            // release: this thread's writes of the child it just finished are
+            // visible to whoever acquires the counter next; acquire: the
+            // second arrival sees the sibling's writes
+            const int old = arrive_acq_rel(&bd[node].flag);
             if (old == 0) break;                    // first arrival: the sibling finishes
-            __threadfence();
             const int cl = __ldcg(&tr[node].child_left);
             const int cr = __ldcg(&tr[node].child_right);
             if (cl < 0 || cr < 0 || cl >= L.n_internal + L.n || cr >= L.n_internal + L.n) {

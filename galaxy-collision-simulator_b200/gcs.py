@@ -108,6 +108,9 @@ def lib() -> C.CDLL:
         "gcs_direct_accels_fp64": (C.c_int, [P, C.POINTER(Params), i32, C.POINTER(i64), i64,
                                              C.POINTER(C.c_double)]),
         "gcs_count_interactions": (C.c_int, [P, C.POINTER(Params), C.POINTER(C.c_uint64)]),
+        "gcs_autotune": (C.c_int, [P, C.POINTER(Params), C.POINTER(C.c_double)]),
+        "gcs_set_group_width": (C.c_int, [P, i32]),
+        "gcs_group_width": (i32, [P]),
         "gcs_dropin_set_params": (C.c_int, [C.POINTER(Params)]),
         "gcs_dropin_context": (P, []),
         "gcs_dropin_device_stars": (P, []),
@@ -278,6 +281,22 @@ class Context:
         out = (C.c_double * 6)()
         self.check(self.L.gcs_diagnostics(self._h, segment, out))
         return np.array(out[:])
+
+    def autotune(self, p: Params) -> tuple[Params, float]:
+        """Fastest (leaf_size <= p.leaf_size, walk_batch, walk_blocks_per_sm)
+        on the current state; the context keeps the fastest group width."""
+        q = Params()
+        C.memmove(C.byref(q), C.byref(p), C.sizeof(Params))
+        ms = C.c_double()
+        self.check(self.L.gcs_autotune(self._h, C.byref(q), C.byref(ms)))
+        return q, ms.value
+
+    @property
+    def group_width(self) -> int:
+        return int(self.L.gcs_group_width(self._h))
+
+    def set_group_width(self, w: int) -> None:
+        self.check(self.L.gcs_set_group_width(self._h, w))
 
     def count_interactions(self, p: Params, warp_evals: bool = False):
         """(monopole terms, particle terms)[, warp node evals, warp source evals,

@@ -103,6 +103,12 @@ int gcs_set_segments(gcs_ctx* ctx, int32_t num_segments, const int64_t* counts);
 int64_t gcs_num_particles(const gcs_ctx* ctx);
 int32_t gcs_num_segments(const gcs_ctx* ctx);
 
+/* Targets per walk group (8..32, default 32): the walk's warps each take a
+ * run of this many consecutive sorted particles of one segment.  Results do
+ * not depend on it (each target's terms are its own walk's); speed does. */
+int gcs_set_group_width(gcs_ctx* ctx, int32_t width);
+int32_t gcs_group_width(const gcs_ctx* ctx);
+
 /* ---- particle data ------------------------------------------------------ */
 /* Copy host Stars into particles [offset, offset+n) (host may be pageable or
  * pinned); the reference's cuda_upload_initial_stars (cuda_engine.cu:342-352). */
@@ -224,6 +230,14 @@ int gcs_diagnostics(gcs_ctx* ctx, int32_t segment, double out[6]);
  * global memory}, then {node evaluations opened by every active lane, node
  * evaluations accepted by every active lane}. */
 int gcs_count_interactions(gcs_ctx* ctx, const gcs_params* p, uint64_t out[8]);
+/* Autotuner: times the walk on the current state for leaf sizes
+ * {1,2,4,8,16,32} up to p->leaf_size (the caller's "leaf <= L"), pop
+ * batches {16,32}, group widths {32,16} and two occupancies, then writes the
+ * fastest leaf_size / walk_batch / walk_blocks_per_sm into *p and keeps the
+ * fastest group width on the context.  It runs bounds..aggregate once (the
+ * particle arrays end in this step's Morton order, values unchanged) and
+ * the walk repeatedly; best_walk_ms (may be NULL) receives the best time. */
+int gcs_autotune(gcs_ctx* ctx, gcs_params* p, double* best_walk_ms);
 /* FP64 direct-sum accelerations (excluding only i == j) at `n_targets`
  * sorted positions `targets` of one segment; result as double[3*n_targets].
  * Reads the current positions; eps^2 and G from p. */

@@ -154,6 +154,29 @@ def test_walk_batch_sizes_agree(gcs_mod, stars, batch):
         _assert_acc(a2[:, :3], a1[:, :3])
 
 
+def test_group_width_and_autotune(gcs_mod, oracle_mod, stars):
+    """Group width changes only the order of the sums; the autotuner returns
+    settings within the caller's leaf bound whose results match the oracle."""
+    gcs = gcs_mod
+    with _ctx(gcs, stars) as ctx:
+        p = _params(gcs, leaf_size=8)
+        ctx.run_stages(p, gcs.STAGE_BOUNDS, gcs.STAGE_WALK)
+        a32 = ctx.read(gcs.BUF_ACCEL)
+        ctx.set_group_width(16)
+        assert ctx.group_width == 16
+        ctx.run_stages(p, gcs.STAGE_WALK, gcs.STAGE_WALK)
+        _assert_acc(ctx.read(gcs.BUF_ACCEL)[:, :3], a32[:, :3], "width 16 vs 32")
+        with pytest.raises(gcs.GcsError):
+            ctx.set_group_width(4)
+        q, ms = ctx.autotune(_params(gcs, leaf_size=8))
+        assert 1 <= q.leaf_size <= 8 and q.walk_batch in (16, 32) and ms > 0
+        ctx.run_stages(q, gcs.STAGE_BOUNDS, gcs.STAGE_WALK)
+        ref = oracle_mod.walk(ctx.read(gcs.BUF_POS), ctx.read(gcs.BUF_NODES), q.G, q.epsilon_sq, q.theta,
+                              q.leaf_size)
+        _assert_acc(ctx.read(gcs.BUF_ACCEL)[:, :3], ref[:, :3], "autotuned")
+        assert ctx.device_status() == 0
+
+
 def test_integrate_bitexact(gcs_mod, oracle_mod, stars):
     gcs = gcs_mod
     with _ctx(gcs, stars) as ctx:
