@@ -641,7 +641,7 @@ int gcs_autotune(gcs_ctx* c, gcs_params* p, double* best_walk_ms) {
     GCS_CUDA(c, cudaEventCreate(&e1));
     const int widths[] = {32, 16};
     const int leaves[] = {1, 2, 4, 8, 16, 32};
-    const int batches[] = {16, 32};
+    const int batches[] = {16, 32, 64};
     const int occupancy[] = {0, 4};
     gcs_params best = *p;
     int best_width = c->group_width;

@@ -100,8 +100,9 @@ struct WalkParams {
 };
 // Global-memory stack entries (int2) per walk warp: the shared-memory stack
 // spills its bottom here.  A round adds at most `batch` entries per tree
-// level, so 4096 covers batch 32 on trees 128 levels deep.
-constexpr int kWalkGlobalStack = 4096;
+// level, so 8192 covers batch 64 on trees 128 levels deep.
+constexpr int kWalkGlobalStack = 8192;
+constexpr int kWalkMaxBatch = 64;  // nodes popped per walk round
 void launch_walk(const Layout& L, const WalkParams& wp, const float4* pos,
                  const BvhNodeTraverse* tr, const WalkGroup* groups, int n_groups,
                  float4* acc, uint32_t* queue, uint32_t* status, int blocks_per_sm,

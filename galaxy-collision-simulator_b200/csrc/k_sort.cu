@@ -36,6 +36,7 @@ constexpr uint32_t kFlagAggregate = 1u << 30;
 constexpr uint32_t kFlagInclusive = 2u << 30;
 constexpr uint32_t kCountMask = (1u << 30) - 1;
 constexpr uint32_t kSpinLimit = 1u << 22;
+constexpr int kLookWindow = 8;
 
 struct SortSmem {
     uint64_t keys[kSortTile];
@@ -138,25 +139,41 @@ onesweep_kernel(Layout L, int shift, const uint64_t* __restrict__ keys_in,
     S.tstart[t] = tstart;
 
     // ---- decoupled look-back for digit t
+    // Predecessors are read kLookWindow at a time (independent loads in
+    // flight together), nearest first, until an inclusive prefix is found;
+    // an empty slot (a tile that has not published yet) restarts the window
+    // there after a short sleep.
     uint32_t excl = 0;
     if (tile > 0) {
         int64_t prev = (int64_t)tile - 1;
         uint32_t spins = 0;
         while (prev >= 0) {
-            const uint32_t v = lb[prev * kRadix + t];
-            const uint32_t flag = v & ~kCountMask;
-            if (flag == 0u) {
+            uint32_t v[kLookWindow];
+#pragma unroll
+            for (int k = 0; k < kLookWindow; ++k) v[k] = prev - k >= 0 ? lb[(prev - k) * kRadix + t] : 0u;
+            int k = 0;
+            bool done = false;
+            for (; k < kLookWindow && prev - k >= 0; ++k) {
+                const uint32_t flag = v[k] & ~kCountMask;
+                if (flag == 0u) break;
+                excl += v[k] & kCountMask;
+                if (flag == kFlagInclusive) {
+                    done = true;
+                    break;
+                }
+            }
+            if (done) break;
+            if (k < kLookWindow && prev - k >= 0) {  // stopped at an empty slot
+                prev -= k;
                 if (++spins > kSpinLimit) {
                     S.bad = 1;
                     atomicOr(status, GCS_DEV_SORT_LOOKBACK_TIMEOUT);
                     break;
                 }
-                __nanosleep(64);
+                __nanosleep(32);
                 continue;
             }
-            excl += v & kCountMask;
-            if (flag == kFlagInclusive) break;
-            --prev;
+            prev -= k;
         }
         lb[(int64_t)tile * kRadix + t] = kFlagInclusive | ((excl + total) & kCountMask);
     }

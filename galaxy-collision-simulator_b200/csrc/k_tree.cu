@@ -33,6 +33,14 @@ __device__ __forceinline__ int arrive_acq_rel(int32_t* flag) {
     asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], 1;" : "=r"(old) : "l"(flag) : "memory");
     return old;
 }
+__device__ __forceinline__ int arrive_relaxed(int32_t* flag) {
+    int old;
+    asm volatile("atom.relaxed.gpu.global.add.s32 %0, [%1], 1;" : "=r"(old) : "l"(flag) : "memory");
+    return old;
+}
+// Acquire side of a relaxed arrival (the fence makes the sibling's writes,
+// released by its own acq_rel arrival, visible to the loads that follow).
+__device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 
 // Common prefix length of sorted keys i and j of one segment (local indices);
 // -1 when j falls outside the segment.
@@ -135,12 +143,17 @@ __device__ __forceinline__ ChildData load_child(int c, int n_internal, const flo
     return r;
 }
 
-__global__ void aggregate_kernel(Layout L, const float4* __restrict__ pos,
+__global__ void __launch_bounds__(256, 4)
+aggregate_kernel(Layout L, const float4* __restrict__ pos,
                                  BvhNodeTraverse* __restrict__ tr, BvhNodeBuild* __restrict__ bd,
                                  double4* __restrict__ com64, const int32_t* __restrict__ leaf_parent,
                                  int com_fp64, uint32_t* __restrict__ status) {
     const bool fp64 = com_fp64 != 0;
     for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < L.n; g += gridDim.x * blockDim.x) {
+        // The node this thread has just finished (first the leaf itself) is
+        // carried in registers; at each parent only the sibling is loaded.
+        int from = L.n_internal + g;
+        ChildData mine = load_child(from, L.n_internal, pos, tr, bd, com64, fp64);
         int node = __ldg(leaf_parent + g);
         int levels = 0;
         while (node >= 0) {
@@ -150,19 +163,32 @@ __global__ void aggregate_kernel(Layout L, const float4* __restrict__ pos,
                 atomicOr(status, GCS_DEV_TREE_MALFORMED);
                 break;
             }
+            // links come from the build launch: fetch them before the arrival
+            const int cl = __ldg(&tr[node].child_left);
+            const int cr = __ldg(&tr[node].child_right);
+            const int up = __ldg(&bd[node].parent);
             // release: this thread's writes of the child it just finished are
             // visible to whoever acquires the counter next; acquire: the
             // second arrival sees the sibling's writes
-            const int old = arrive_acq_rel(&bd[node].flag);
+            // At the leaf level this thread has written nothing, so its
+            // arrival needs no release; it acquires only if it arrives second.
+            int old;
+            if (levels == 1) {
+                old = arrive_relaxed(&bd[node].flag);
+                if (old != 0) fence_acq_rel();
+            } else {
+                old = arrive_acq_rel(&bd[node].flag);
+            }
             if (old == 0) break;                    // first arrival: the sibling finishes
-            const int cl = __ldcg(&tr[node].child_left);
-            const int cr = __ldcg(&tr[node].child_right);
-            if (cl < 0 || cr < 0 || cl >= L.n_internal + L.n || cr >= L.n_internal + L.n) {
+            if (cl < 0 || cr < 0 || cl >= L.n_internal + L.n || cr >= L.n_internal + L.n ||
+                (cl != from && cr != from)) {
                 atomicOr(status, GCS_DEV_TREE_MALFORMED);
                 break;
             }
-            const ChildData A = load_child(cl, L.n_internal, pos, tr, bd, com64, fp64);
-            const ChildData B = load_child(cr, L.n_internal, pos, tr, bd, com64, fp64);
+            const bool left = cl == from;
+            const ChildData other = load_child(left ? cr : cl, L.n_internal, pos, tr, bd, com64, fp64);
+            const ChildData& A = left ? mine : other;   // left child
+            const ChildData& B = left ? other : mine;   // right child
             const float3 lo = make_float3(fminf(A.lo.x, B.lo.x), fminf(A.lo.y, B.lo.y),
                                           fminf(A.lo.z, B.lo.z));
             const float3 hi = make_float3(fmaxf(A.hi.x, B.hi.x), fmaxf(A.hi.y, B.hi.y),
@@ -194,7 +220,20 @@ __global__ void aggregate_kernel(Layout L, const float4* __restrict__ pos,
             float4* b4 = reinterpret_cast<float4*>(bd + node);
             b4[0] = make_float4(lo.x, lo.y, lo.z, hi.x);
             reinterpret_cast<float2*>(b4 + 1)[0] = make_float2(hi.y, hi.z);
-            node = __ldcg(&bd[node].parent);
+            ChildData next;
+            next.lo = lo;
+            next.hi = hi;
+            next.com = com;
+            next.m = m;
+            if (fp64) {
+                const bool pos_mass = m > 0.0f;
+                next.md = pos_mass ? A.md + B.md : 0.0;
+                next.mx = pos_mass ? make_double3(A.mx.x + B.mx.x, A.mx.y + B.mx.y, A.mx.z + B.mx.z)
+                                   : make_double3(0.0, 0.0, 0.0);
+            }
+            mine = next;
+            from = node;
+            node = up;
         }
     }
 }

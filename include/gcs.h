@@ -68,7 +68,7 @@ typedef struct gcs_params {
     int32_t recolor;    /* 1: the reference's speed colour map for types 0/2 */
     int32_t com_fp64;   /* 1: node centres of mass from FP64 sums;
                            0: the reference's FP32 pairwise formula */
-    int32_t walk_batch; /* nodes fetched per stack pop, 1..32 (0 = tuned default) */
+    int32_t walk_batch; /* nodes fetched per stack pop, 1..64 (0 = default 32) */
     int32_t walk_blocks_per_sm; /* persistent walk occupancy (0 = default) */
     int32_t with_potential; /* 1: the walk also sums potentials (ACCEL .w) */
     int32_t reserved[3];
@@ -232,7 +232,7 @@ int gcs_diagnostics(gcs_ctx* ctx, int32_t segment, double out[6]);
 int gcs_count_interactions(gcs_ctx* ctx, const gcs_params* p, uint64_t out[8]);
 /* Autotuner: times the walk on the current state for leaf sizes
  * {1,2,4,8,16,32} up to p->leaf_size (the caller's "leaf <= L"), pop
- * batches {16,32}, group widths {32,16} and two occupancies, then writes the
+ * batches {16,32,64}, group widths {32,16} and two occupancies, then writes the
  * fastest leaf_size / walk_batch / walk_blocks_per_sm into *p and keeps the
  * fastest group width on the context.  It runs bounds..aggregate once (the
  * particle arrays end in this step's Morton order, values unchanged) and

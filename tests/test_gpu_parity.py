@@ -143,7 +143,7 @@ def test_walk_matches_oracle(gcs_mod, oracle_mod, stars, theta, leaf):
         assert ctx.device_status() == 0
 
 
-@pytest.mark.parametrize("batch", [1, 4, 32])
+@pytest.mark.parametrize("batch", [1, 4, 32, 33, 64])
 def test_walk_batch_sizes_agree(gcs_mod, stars, batch):
     gcs = gcs_mod
     with _ctx(gcs, stars) as ctx:
@@ -169,7 +169,7 @@ def test_group_width_and_autotune(gcs_mod, oracle_mod, stars):
         with pytest.raises(gcs.GcsError):
             ctx.set_group_width(4)
         q, ms = ctx.autotune(_params(gcs, leaf_size=8))
-        assert 1 <= q.leaf_size <= 8 and q.walk_batch in (16, 32) and ms > 0
+        assert 1 <= q.leaf_size <= 8 and q.walk_batch in (16, 32, 64) and ms > 0
         ctx.run_stages(q, gcs.STAGE_BOUNDS, gcs.STAGE_WALK)
         ref = oracle_mod.walk(ctx.read(gcs.BUF_POS), ctx.read(gcs.BUF_NODES), q.G, q.epsilon_sq, q.theta,
                               q.leaf_size)
