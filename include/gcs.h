@@ -158,7 +158,8 @@ int gcs_device_status(gcs_ctx* ctx, uint32_t* status, int32_t clear);
  * before this step's sort), NODES BvhNodeTraverse, BUILD BvhNodeBuild,
  * LEAF_PARENT i32, ACCEL float4 (ax,ay,az,potential), POS float4 (x,y,z,m),
  * VEL float4 (vx,vy,vz, bits of type|r|g|b), BOUNDS float2 per segment,
- * KEYS_UNSORTED u64 (encode output). */
+ * KEYS_UNSORTED u64 (encode output; valid until the sort stage runs, which
+ * uses that buffer for its passes). */
 #define GCS_BUF_KEYS          0
 #define GCS_BUF_INDEX         1
 #define GCS_BUF_NODES         2
