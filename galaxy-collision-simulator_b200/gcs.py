@@ -111,6 +111,7 @@ def lib() -> C.CDLL:
         "gcs_autotune": (C.c_int, [P, C.POINTER(Params), C.POINTER(C.c_double)]),
         "gcs_set_group_width": (C.c_int, [P, i32]),
         "gcs_group_width": (i32, [P]),
+        "gcs_sort_pairs_static": (C.c_int, [P, P, P, P, i64, P, P]),
         "gcs_dropin_set_params": (C.c_int, [C.POINTER(Params)]),
         "gcs_dropin_context": (P, []),
         "gcs_dropin_device_stars": (P, []),

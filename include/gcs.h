@@ -239,6 +239,25 @@ int gcs_count_interactions(gcs_ctx* ctx, const gcs_params* p, uint64_t out[8]);
  * particle arrays end in this step's Morton order, values unchanged) and
  * the walk repeatedly; best_walk_ms (may be NULL) receives the best time. */
 int gcs_autotune(gcs_ctx* ctx, gcs_params* p, double* best_walk_ms);
+/* Allocation-free sort (no counterpart in the reference): a stable sort of
+ * n <= 1,048,576 (u64 key, u32 value) pairs by the whole key, for callers
+ * that cannot allocate device memory where they sort (a real-time loop or
+ * host callback that must not trigger an allocation's implicit device
+ * synchronisation, or a plug-in whose host application owns the device
+ * memory budget).  All pointers are device memory owned by the caller:
+ * keys/vals hold the pairs and receive the sorted pairs; keys_alt/vals_alt
+ * are the same length and are overwritten by the passes; status (may be
+ * NULL) receives GCS_DEV_SORT_LOOKBACK_TIMEOUT if a pass gave up.  The
+ * histograms and look-back state live in one static device array of about
+ * 2.1 MB that every GPU loading this library keeps until exit; no call
+ * allocates.  Each call clears that array on `stream` (a cudaStream_t, NULL
+ * = legacy default) before using it, so calls ordered on the GPU are
+ * independent, but calls that overlap on the GPU race on it.  The first
+ * call on a device looks up the array's device address (with that device
+ * current) - make it before any stream capture.  Larger n returns
+ * GCS_ERR_CAPACITY; the call is asynchronous. */
+int gcs_sort_pairs_static(uint64_t* keys, uint32_t* vals, uint64_t* keys_alt, uint32_t* vals_alt,
+                          int64_t n, uint32_t* status, void* stream);
 /* FP64 direct-sum accelerations (excluding only i == j) at `n_targets`
  * sorted positions `targets` of one segment; result as double[3*n_targets].
  * Reads the current positions; eps^2 and G from p. */
