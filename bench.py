@@ -61,7 +61,16 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--batched-count", type=int, default=256)
+    ap.add_argument("--batched-steps", type=int, default=10)
+    ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--served-requests", type=int, default=48)
+    ap.add_argument("--served-step-scale", type=float, default=0.05)
+    ap.add_argument("--served-loads", type=lambda v: [float(x) for x in v.split(",")], default=[0.5, 0.9],
+                    help="offered loads as fractions of the batched throughput")
     return ap.parse_args()
 
 
@@ -208,6 +217,198 @@ def ref_gpu_rate(stars, steps=3):
                     "device time, same GPU"}
 
 
+def accuracy(gcs, ctx, p, stars, n_sub=65536, seed=0):
+    """Median / p99 relative force error against an FP64 direct sum (GPU,
+    excluding only i == j) on a seeded subset of targets, for this engine
+    and - when oracle/_ref was built - for the reference's own GPU walk at
+    the same theta on the same snapshot (its leaf size is 1)."""
+    import numpy as np  # noqa: PLC0415
+    ctx.upload(stars)
+    ctx.compute_accels(p)
+    acc = ctx.read(gcs.BUF_ACCEL)[:, :3].astype(np.float64)
+    keys = ctx.read(gcs.BUF_KEYS)
+    n = len(stars)
+    rng = np.random.default_rng(seed)
+    tg = np.sort(rng.choice(n, size=min(n_sub, n), replace=False))
+    exact = ctx.direct_fp64(p, tg)
+    norm = np.linalg.norm(exact, axis=1)
+
+    def stats(a):
+        e = np.linalg.norm(a[tg] - exact, axis=1) / norm
+        return {"median": float(np.median(e)), "p99": float(np.percentile(e, 99))}
+
+    out = {"subset": int(len(tg)), "theta": p.theta, "leaf_size": p.leaf_size, "engine": stats(acc)}
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle  # noqa: PLC0415
+    if oracle.ref_lib("ref_cuda") is not None:
+        pos, _ = gcs.pos_vel_from_stars(stars)
+        lo, hi = float(pos[:, :3].min()), float(pos[:, :3].max())
+        ref = oracle.RefCuda(n)
+        try:
+            ref.set_theta(p.theta)
+            ref.upload(stars)
+            ref.step_device(p.G, p.epsilon_sq, 0.0, lo, hi)
+            same_order = bool(np.array_equal(ref.read(0), keys))
+            racc = ref.read(4).astype(np.float64)
+        finally:
+            ref.close()
+        if same_order:  # identical keys -> identical stable permutation
+            out["reference_gpu"] = stats(racc)
+            out["reference_gpu"]["leaf_size"] = 1
+        else:
+            out["reference_gpu"] = {"unavailable": "sorted orders differ"}
+    return out
+
+
+def _tune(gcs, ctx, leaf_max=32):
+    """Autotuned parameters on the context's current state (leaf >= 4, as in
+    the 1M run), then the state is the caller's to re-upload."""
+    q = make_params(gcs, leaf_max, 0)
+    q.tune_leaf_min = 4
+    p, _ = ctx.autotune(q)
+    return p
+
+
+def batched_bench(gcs, torch, args):
+    """256 uneven scenarios: all advanced together (segments of one context,
+    one launch per stage, graph-captured step) versus the same scenarios one
+    at a time through the same engine (one segment, graph-captured step).
+    Device time of K steps after W warm-up steps, both ways."""
+    import workloads  # noqa: PLC0415
+    scen = workloads.batched_scenarios(count=args.batched_count)
+    t0 = time.perf_counter()
+    stars = [s.stars(gcs) for s in scen]
+    gen_s = time.perf_counter() - t0
+    counts = [len(s) for s in stars]
+    total = sum(counts)
+    allst = np.concatenate(stars)
+    stream = torch.cuda.Stream()
+    K, W = args.batched_steps, max(3, args.warmup)
+    with gcs.Context(total, max_segments=len(scen)) as ctx:
+        ctx.set_stream(stream.cuda_stream)
+        ctx.set_segments(counts)
+        ctx.upload(allst)
+        p = _tune(gcs, ctx)
+        width = ctx.group_width
+        ctx.upload(allst)
+        ctx.set_graphs(True)
+        for _ in range(W):
+            ctx.step(p)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        stream.synchronize()
+        e0.record(stream)
+        for _ in range(K):
+            ctx.step(p)
+        e1.record(stream)
+        e1.synchronize()
+        t_batched = e0.elapsed_time(e1) / 1e3
+        if ctx.device_status():
+            raise RuntimeError("device status raised in the batched run")
+        builds = ctx.graph_builds
+    seq_s = 0.0
+    with gcs.Context(max(counts)) as ctx:
+        ctx.set_stream(stream.cuda_stream)
+        ctx.set_group_width(width)
+        ctx.set_graphs(True)
+        for st in stars:
+            ctx.set_segments([len(st)])
+            ctx.upload(st)
+            for _ in range(W):
+                ctx.step(p)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(K):
+                ctx.step(p)
+            e1.record(stream)
+            e1.synchronize()
+            seq_s += e0.elapsed_time(e1) / 1e3
+        if ctx.device_status():
+            raise RuntimeError("device status raised in the one-at-a-time run")
+    rb = total * K / t_batched
+    rs = total * K / seq_s
+    return {"workload": "%d independent two-galaxy collisions, N log-uniform in [4096, 262144] (total %d), "
+                        "q U[0.2,1], impact U[0,15], incline U[0,90] deg, speed U[0.3,0.8], seeds 0..%d; "
+                        "theta=0.5, eps=0.02, dt=0.0025" % (len(scen), total, len(scen) - 1),
+            "timed_steps": K, "warmup": W, "steps_of_recipe": 500,
+            "batched": {"value": rb, "unit": "particle-steps/s", "ms_per_step": t_batched * 1e3 / K,
+                        "graph_builds": builds},
+            "one_at_a_time": {"value": rs, "unit": "particle-steps/s", "seconds": seq_s,
+                              "path": "one segment per context layout, graph-captured step, same parameters"},
+            "speedup": rb / rs, "leaf_size": p.leaf_size, "walk_batch": p.walk_batch, "group_width": width,
+            "ic_seconds": gen_s}
+
+
+def _serve(gcs, p, reqs, stars, max_segments, budget):
+    """Drive a server with requests arriving at their wall-clock times; returns
+    latencies (ms) and the makespan (first arrival to last completion)."""
+    srv = gcs.Server(p, max_particles=(1 << 30) - 1, max_segments=max_segments, hbm_budget_bytes=budget)
+    try:
+        lat, queued = [], []
+        t0 = time.perf_counter()
+        i, done, R = 0, 0, len(reqs)
+        peak = [0, 0]
+        while done < R:
+            now = time.perf_counter() - t0
+            while i < R and reqs[i].arrival_s <= now:
+                srv.submit(i, stars[i], reqs[i].steps)
+                i += 1
+            q, r, f = srv.counts()
+            if q + r == 0 and f == 0:
+                if i < R:
+                    time.sleep(max(0.0, min(0.001, reqs[i].arrival_s - now)))
+                continue
+            if q + r:
+                res = srv.tick()
+                peak = [max(peak[0], res[0]), max(peak[1], res[1])]
+            while (x := srv.pop(with_stars=False)) is not None:
+                info = x[0]
+                if info.status != 0:
+                    raise RuntimeError("served scenario %d failed with status %d" % (info.id, info.status))
+                lat.append(info.latency_ms)
+                queued.append(info.queued_ms)
+                done += 1
+        makespan = time.perf_counter() - t0 - reqs[0].arrival_s
+        cap = srv.capacity
+    finally:
+        srv.close()
+    return lat, queued, makespan, peak, cap
+
+
+def served_bench(gcs, torch, args, batched_rate):
+    """Poisson request streams at offered loads that are fractions of the
+    batched throughput, served by continuous batching and by the plain
+    one-at-a-time path (the same server with one slot)."""
+    import workloads  # noqa: PLC0415
+    free, _ = torch.cuda.mem_get_info()
+    budget = min(150e9, 0.8 * free)
+    base = workloads.serving_requests(args.served_requests, 1.0, step_scale=args.served_step_scale)
+    stars = [s.stars(gcs) for s in base]
+    work = [s.n * s.steps for s in base]
+    mean_work = float(np.mean(work))
+    p = make_params(gcs, 8, 0)
+    with gcs.Context(max(len(s) for s in stars)) as ctx:
+        ctx.upload(stars[int(np.argmax([len(s) for s in stars]))])
+        p = _tune(gcs, ctx)
+    out = {"workload": "%d requests, Poisson arrivals, N log-uniform in [8192, 1048576], steps uniform in "
+                       "[100, 2000] x %.3g, other draws as the batched stream; theta=0.5, eps=0.02, dt=0.0025"
+                       % (len(base), args.served_step_scale),
+           "hbm_budget_bytes": budget, "leaf_size": p.leaf_size, "loads": []}
+    for rho in args.served_loads:
+        rate = rho * batched_rate / mean_work
+        reqs = workloads.serving_requests(args.served_requests, rate, step_scale=args.served_step_scale)
+        row = {"offered_fraction_of_batched_throughput": rho, "rate_req_per_s": rate,
+               "offered_particle_steps_per_s": rate * mean_work}
+        for name, slots in (("continuous_batching", 256), ("one_at_a_time", 1)):
+            lat, qd, span, peak, cap = _serve(gcs, p, reqs, stars, slots, budget)
+            row[name] = {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                         "mean_queue_ms": float(np.mean(qd)),
+                         "throughput": float(sum(work) / span), "unit": "particle-steps/s",
+                         "makespan_s": span, "peak_resident_scenarios": peak[0],
+                         "peak_resident_particles": peak[1], "capacity_particles": cap}
+        out["loads"].append(row)
+    return out
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return 0
@@ -280,8 +481,15 @@ def main():
         p = make_params(gcs, args.leaf, args.batch)
     else:
         # the recipe's "leaf <= 32": the autotuner picks leaf size, pop batch,
-        # group width and occupancy on the initial state (outside the timing)
-        p, tune_ms = ctx.autotune(make_params(gcs, args.leaf if args.leaf > 0 else 32, args.batch))
+        # group width and occupancy on the initial state (outside the timing);
+        # leaf sizes 1 and 2 give exactly the reference's terms, larger ones
+        # sum small opened nodes exactly, which lowers the median error below
+        # the reference's; the search starts at 4 so the accuracy condition
+        # (median error no worse than the reference's at the same theta)
+        # holds with a margin, not only to rounding
+        q = make_params(gcs, args.leaf if args.leaf > 0 else 32, args.batch)
+        q.tune_leaf_min = 4
+        p, tune_ms = ctx.autotune(q)
         tuned = {"leaf_size": p.leaf_size, "walk_batch": p.walk_batch, "blocks_per_sm": p.walk_blocks_per_sm,
                  "group_width": ctx.group_width, "walk_ms": tune_ms}
     ctx.upload(stars)
@@ -368,11 +576,19 @@ def main():
             "e2e": e2e, "roofline": roofline, "clocks": clocks, "gpu_launches": launches_per_step * args.steps,
             "device_status": status}
     if rank == 0 and world == 1:
+        if not args.no_accuracy:
+            line["accuracy"] = accuracy(gcs, ctx, p, stars)
         if not args.no_ref_gpu:
             line["ref_gpu"] = ref_gpu_rate(stars)
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_reference_rate(stars, args.cpu_seconds)
     ctx.close()
+    if rank == 0 and world == 1:
+        if not args.no_batched:
+            line["batched"] = batched_bench(gcs, torch, args)
+        if not args.no_served:
+            rate = line["batched"]["batched"]["value"] if "batched" in line else value
+            line["served"] = served_bench(gcs, torch, args, rate)
     if rank == 0:
         print(json.dumps(line))
     if dist is not None:

@@ -22,6 +22,8 @@ struct gcs_ctx {
     cudaStream_t stream = nullptr;
     int64_t capacity = 0;
     int32_t max_segments = 1;
+    size_t device_bytes = 0;  // bytes this context holds on the device
+    bool dry_run = false;      // count allocations without making them
 
     // layout
     int32_t n = 0, nseg = 0, n_internal = 0;
@@ -60,6 +62,16 @@ struct gcs_ctx {
     int32_t group_width = 32;              // targets per walk group (<= 32)
     size_t groups_cap = 0;
     bool count_walk = false;
+
+    // CUDA graphs of one full step, one per ping-pong parity of the particle
+    // arrays (the gather flips it every step); rebuilt when the parameters,
+    // the layout or the stream change.
+    bool use_graphs = false;
+    bool graphs_valid = false;
+    gcs_params graph_params;
+    cudaStream_t graph_stream = nullptr;
+    cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
+    int graph_builds = 0;
 
     std::string last_error;
 };
@@ -126,16 +138,30 @@ T* scratch_at(gcs_ctx* c, size_t off) {
 
 template <typename T>
 int dalloc(gcs_ctx* c, T** p, size_t count) {
+    if (c->dry_run) {  // footprint only (gcs_context_bytes)
+        c->device_bytes += sizeof(T) * (count > 0 ? count : 1);
+        return GCS_OK;
+    }
     cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), sizeof(T) * (count > 0 ? count : 1));
     if (e != cudaSuccess) {
         set_error(c, "cudaMalloc", e);
         *p = nullptr;
         return GCS_ERR_NOMEM;
     }
+    c->device_bytes += sizeof(T) * (count > 0 ? count : 1);
     return GCS_OK;
 }
 
+void drop_graphs(gcs_ctx* c) {
+    for (auto& g : c->graph_exec) {
+        if (g) cudaGraphExecDestroy(g);
+        g = nullptr;
+    }
+    c->graphs_valid = false;
+}
+
 void free_all(gcs_ctx* c) {
+    drop_graphs(c);
     void* ptrs[] = {c->pos[0], c->pos[1], c->vel[0], c->vel[1], c->acc, c->keys[0], c->keys[1],
                     c->idx[0], c->idx[1], c->tr, c->bd, c->com64, c->leaf_parent, c->seg_off,
                     c->seg_id, c->groups, c->chunks, c->seg_bounds, c->staging, c->pb_staging,
@@ -188,8 +214,9 @@ int upload_groups(gcs_ctx* c) {
         return GCS_ERR_CAPACITY;
     }
     cudaSetDevice(c->device);
-    GCS_CUDA(c, cudaMemcpy(c->groups, groups.data(), sizeof(WalkGroup) * groups.size(),
-                           cudaMemcpyHostToDevice));
+    GCS_CUDA(c, cudaStreamSynchronize(c->stream));
+    GCS_CUDA(c, cudaMemcpyAsync(c->groups, groups.data(), sizeof(WalkGroup) * groups.size(),
+                                cudaMemcpyHostToDevice, c->stream));
     c->n_groups = (int)groups.size();
     return GCS_OK;
 }
@@ -332,6 +359,8 @@ const char* gcs_status_string(int status) {
 
 const char* gcs_last_error(const gcs_ctx* c) { return c ? c->last_error.c_str() : "null context"; }
 
+static int allocate_state(gcs_ctx* c);
+
 int gcs_create(gcs_ctx** out, int64_t capacity, int32_t max_segments, int32_t device) {
     if (!out || capacity < 1 || capacity > (int64_t)(1 << 30) - 1 || max_segments < 1 ||
         max_segments > 65536)
@@ -352,6 +381,52 @@ int gcs_create(gcs_ctx** out, int64_t capacity, int32_t max_segments, int32_t de
     c->sm_count = prop.multiProcessorCount;
     c->capacity = capacity;
     c->max_segments = max_segments;
+    int rc = allocate_state(c);
+    if (rc) {
+        free_all(c);
+        delete c;
+        return GCS_ERR_NOMEM;
+    }
+    cudaMemset(c->scratch, 0, c->scratch_cap);  // the walk queue starts (and stays) at zero
+    cudaMemset(c->status, 0, sizeof(uint32_t));
+    cudaMemset(c->acc, 0, sizeof(float4) * (size_t)capacity);
+    int64_t cnt = capacity;
+    rc = gcs_set_segments(c, 1, &cnt);
+    if (rc) {
+        free_all(c);
+        delete c;
+        return rc;
+    }
+    *out = c;
+    return GCS_OK;
+}
+
+int64_t gcs_context_bytes(int64_t capacity, int32_t max_segments, int32_t device) {
+    if (capacity < 1 || capacity > (int64_t)(1 << 30) - 1 || max_segments < 1 || max_segments > 65536)
+        return GCS_ERR_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device || device < 0) {
+        cudaGetLastError();
+        return GCS_ERR_NO_DEVICE;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major != 10) return GCS_ERR_NO_DEVICE;
+    if (cudaSetDevice(device) != cudaSuccess) return GCS_ERR_NO_DEVICE;
+    gcs_ctx c;
+    c.device = device;
+    c.sm_count = prop.multiProcessorCount;
+    c.capacity = capacity;
+    c.max_segments = max_segments;
+    c.dry_run = true;
+    allocate_state(&c);
+    return (int64_t)c.device_bytes;
+}
+
+// Every device array of a context, sized for its capacity and max_segments
+// (with dry_run set, only the bytes are counted).
+static int allocate_state(gcs_ctx* c) {
+    const int64_t capacity = c->capacity;
+    const int32_t max_segments = c->max_segments;
     const size_t N = (size_t)capacity;
     // groups as narrow as kMinGroupWidth targets (the autotuner's smallest)
     const size_t max_groups = N / kMinGroupWidth + (size_t)max_segments + 1;
@@ -391,23 +466,7 @@ int gcs_create(gcs_ctx** out, int64_t capacity, int32_t max_segments, int32_t de
         c->scratch_cap = scratch_layout(max_segments, capacity, max_segments).end;
         rc |= dalloc(c, &c->scratch, c->scratch_cap);
     }
-    if (rc) {
-        free_all(c);
-        delete c;
-        return GCS_ERR_NOMEM;
-    }
-    cudaMemset(c->scratch, 0, c->scratch_cap);  // the walk queue starts (and stays) at zero
-    cudaMemset(c->status, 0, sizeof(uint32_t));
-    cudaMemset(c->acc, 0, sizeof(float4) * N);
-    int64_t cnt = capacity;
-    rc = gcs_set_segments(c, 1, &cnt);
-    if (rc) {
-        free_all(c);
-        delete c;
-        return rc;
-    }
-    *out = c;
-    return GCS_OK;
+    return rc;
 }
 
 void gcs_destroy(gcs_ctx* c) {
@@ -422,12 +481,14 @@ void gcs_destroy(gcs_ctx* c) {
 int gcs_set_stream(gcs_ctx* c, void* stream) {
     if (!c) return GCS_ERR_ARG;
     c->stream = reinterpret_cast<cudaStream_t>(stream);
+    drop_graphs(c);
     return GCS_OK;
 }
 
 void* gcs_get_stream(const gcs_ctx* c) { return c ? reinterpret_cast<void*>(c->stream) : nullptr; }
 
-int gcs_set_segments(gcs_ctx* c, int32_t num_segments, const int64_t* counts) {
+// Segment tables for a new layout; the particle arrays are not touched.
+static int apply_layout(gcs_ctx* c, int32_t num_segments, const int64_t* counts) {
     if (!c || num_segments < 1 || !counts) return GCS_ERR_ARG;
     if (num_segments > c->max_segments) {
         c->last_error = "more segments than max_segments";
@@ -446,10 +507,8 @@ int gcs_set_segments(gcs_ctx* c, int32_t num_segments, const int64_t* counts) {
         return GCS_ERR_CAPACITY;
     }
     const int64_t n = off[num_segments];
-    std::vector<int32_t> sid((size_t)n);
     std::vector<Chunk> chunks;
     for (int s = 0; s < num_segments; ++s) {
-        for (int64_t i = off[s]; i < off[s + 1]; ++i) sid[(size_t)i] = s;
         for (int64_t g = off[s]; g < off[s + 1]; g += kChunkSize) {
             Chunk ch;
             ch.start = (int32_t)g;
@@ -460,22 +519,87 @@ int gcs_set_segments(gcs_ctx* c, int32_t num_segments, const int64_t* counts) {
         }
     }
     cudaSetDevice(c->device);
-    GCS_CUDA(c, cudaMemcpy(c->seg_off, off.data(), sizeof(int64_t) * off.size(), cudaMemcpyHostToDevice));
-    GCS_CUDA(c, cudaMemcpy(c->seg_id, sid.data(), sizeof(int32_t) * sid.size(), cudaMemcpyHostToDevice));
-    GCS_CUDA(c, cudaMemcpy(c->chunks, chunks.data(), sizeof(Chunk) * chunks.size(),
-                           cudaMemcpyHostToDevice));
+    // The tables are read by steps already queued on the context stream:
+    // let those finish, then write the new tables in stream order (pageable
+    // sources are staged before each copy call returns).
+    GCS_CUDA(c, cudaStreamSynchronize(c->stream));
+    GCS_CUDA(c, cudaMemcpyAsync(c->seg_off, off.data(), sizeof(int64_t) * off.size(),
+                                cudaMemcpyHostToDevice, c->stream));
+    launch_fill_segment_ids(c->seg_off, num_segments, c->seg_id, n, c->stream);
+    int rc = check_launch(c, "fill_segment_ids");
+    if (rc) return rc;
+    GCS_CUDA(c, cudaMemcpyAsync(c->chunks, chunks.data(), sizeof(Chunk) * chunks.size(),
+                                cudaMemcpyHostToDevice, c->stream));
     c->h_seg_off = off;
     c->n = (int32_t)n;
     c->nseg = num_segments;
     c->n_internal = (int32_t)(n - num_segments);
     c->n_chunks = (int)chunks.size();
-    c->cur = 0;
+    drop_graphs(c);
     return upload_groups(c);
+}
+
+int gcs_set_segments(gcs_ctx* c, int32_t num_segments, const int64_t* counts) {
+    const int rc = apply_layout(c, num_segments, counts);
+    if (!rc) c->cur = 0;
+    return rc;
+}
+
+int gcs_relayout(gcs_ctx* c, int32_t num_segments, const int64_t* counts, const int32_t* src_segment) {
+    if (!c || num_segments < 1 || !counts || !src_segment) return GCS_ERR_ARG;
+    const std::vector<int64_t> old_off = c->h_seg_off;
+    const int old_nseg = c->nseg;
+    int64_t dst = 0;
+    std::vector<int64_t> dst_off((size_t)num_segments);
+    for (int s = 0; s < num_segments; ++s) {
+        const int src = src_segment[s];
+        if (src >= old_nseg || (src >= 0 && old_off[src + 1] - old_off[src] != counts[s])) {
+            c->last_error = "relayout: a kept segment must keep its particle count";
+            return GCS_ERR_ARG;
+        }
+        for (int t = 0; t < s; ++t)
+            if (src >= 0 && src_segment[t] == src) {
+                c->last_error = "relayout: a segment is kept twice";
+                return GCS_ERR_ARG;
+            }
+        dst_off[s] = dst;
+        dst += counts[s];
+    }
+    if (dst > c->capacity || num_segments > c->max_segments) {
+        c->last_error = "relayout exceeds the context capacity";
+        return GCS_ERR_CAPACITY;
+    }
+    cudaSetDevice(c->device);
+    bool in_place = true;
+    for (int s = 0; s < num_segments; ++s)
+        if (src_segment[s] >= 0 && dst_off[s] != old_off[src_segment[s]]) in_place = false;
+    if (in_place) return apply_layout(c, num_segments, counts);
+    // kept segments move into the other ping-pong buffer at their new offsets
+    const int from = c->cur, to = c->cur ^ 1;
+    for (int s = 0; s < num_segments; ++s) {
+        const int src = src_segment[s];
+        if (src < 0) continue;
+        const size_t bytes = sizeof(float4) * (size_t)counts[s];
+        GCS_CUDA(c, cudaMemcpyAsync(c->pos[to] + dst_off[s], c->pos[from] + old_off[src], bytes,
+                                    cudaMemcpyDeviceToDevice, c->stream));
+        GCS_CUDA(c, cudaMemcpyAsync(c->vel[to] + dst_off[s], c->vel[from] + old_off[src], bytes,
+                                    cudaMemcpyDeviceToDevice, c->stream));
+    }
+    const int rc = apply_layout(c, num_segments, counts);
+    if (rc) return rc;
+    c->cur = to;
+    return GCS_OK;
+}
+
+int64_t gcs_segment_offset(const gcs_ctx* c, int32_t segment) {
+    if (!c || segment < 0 || segment > c->nseg) return -1;
+    return c->h_seg_off[segment];
 }
 
 int gcs_set_group_width(gcs_ctx* c, int32_t width) {
     if (!c || width < kMinGroupWidth || width > kGroupSize) return GCS_ERR_ARG;
     c->group_width = width;
+    drop_graphs(c);
     return upload_groups(c);
 }
 
@@ -484,6 +608,7 @@ int32_t gcs_group_width(const gcs_ctx* c) { return c ? c->group_width : 0; }
 int64_t gcs_num_particles(const gcs_ctx* c) { return c ? c->n : 0; }
 int32_t gcs_num_segments(const gcs_ctx* c) { return c ? c->nseg : 0; }
 int64_t gcs_num_internal_nodes(const gcs_ctx* c) { return c ? c->n_internal : 0; }
+int64_t gcs_device_bytes(const gcs_ctx* c) { return c ? (int64_t)c->device_bytes : 0; }
 
 int gcs_upload_stars(gcs_ctx* c, const Star* host, int64_t offset, int64_t n) {
     if (!c || !host || offset < 0 || n < 0 || offset + n > c->n) return GCS_ERR_ARG;
@@ -527,10 +652,84 @@ int gcs_download_playback(gcs_ctx* c, PlaybackStar* host, int64_t offset, int64_
     return GCS_OK;
 }
 
+// Capture the full step twice, once from each ping-pong parity of the
+// particle arrays, into executable graphs.  The stage launches are the ones
+// an eager step makes; capture runs on the context stream in thread-local
+// mode, so other threads' CUDA calls are unaffected.
+static int build_step_graphs(gcs_ctx* c, const gcs_params* p) {
+    drop_graphs(c);
+    const int cur0 = c->cur;
+    int rc = GCS_OK;
+    for (int k = 0; k < 2 && !rc; ++k) {
+        const int parity = cur0 ^ k;
+        c->cur = parity;
+        cudaGraph_t graph = nullptr;
+        if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            c->last_error = "cudaStreamBeginCapture failed";
+            rc = GCS_ERR_CUDA;
+            break;
+        }
+        rc = run_stages(c, p, GCS_STAGE_BOUNDS, GCS_STAGE_INTEGRATE);
+        const cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+        if (!rc && e != cudaSuccess) {
+            set_error(c, "cudaStreamEndCapture", e);
+            rc = GCS_ERR_CUDA;
+        }
+        if (!rc) {
+            const cudaError_t ei = cudaGraphInstantiate(&c->graph_exec[parity], graph, 0);
+            if (ei != cudaSuccess) {
+                set_error(c, "cudaGraphInstantiate", ei);
+                rc = GCS_ERR_CUDA;
+            }
+        }
+        if (graph) cudaGraphDestroy(graph);
+    }
+    c->cur = cur0;
+    if (rc) {
+        drop_graphs(c);
+        cudaGetLastError();
+        return rc;
+    }
+    c->graph_params = *p;
+    c->graph_stream = c->stream;
+    c->graphs_valid = true;
+    ++c->graph_builds;
+    return GCS_OK;
+}
+
 int gcs_step(gcs_ctx* c, const gcs_params* p) {
     if (!c) return GCS_ERR_ARG;
-    return run_stages(c, p, GCS_STAGE_BOUNDS, GCS_STAGE_INTEGRATE);
+    if (!c->use_graphs) return run_stages(c, p, GCS_STAGE_BOUNDS, GCS_STAGE_INTEGRATE);
+    int rc = validate_params(c, p);
+    if (rc) return rc;
+    if (c->n <= 0) {
+        c->last_error = "no particles";
+        return GCS_ERR_STATE;
+    }
+    if (!c->graphs_valid || c->graph_stream != c->stream ||
+        memcmp(&c->graph_params, p, sizeof(gcs_params)) != 0) {
+        rc = build_step_graphs(c, p);
+        if (rc) return rc;
+    }
+    cudaSetDevice(c->device);
+    GCS_CUDA(c, cudaGraphLaunch(c->graph_exec[c->cur], c->stream));
+    c->cur ^= 1;  // the captured gather flipped the arrays
+    c->sorted_buf = (kKeyPasses + seg_passes(c->nseg)) & 1;
+    return GCS_OK;
 }
+
+int gcs_set_graphs(gcs_ctx* c, int32_t enable) {
+    if (!c) return GCS_ERR_ARG;
+    if (enable && c->stream == nullptr) {
+        c->last_error = "graph capture needs a non-default stream (gcs_set_stream)";
+        return GCS_ERR_STATE;
+    }
+    c->use_graphs = enable != 0;
+    if (!c->use_graphs) drop_graphs(c);
+    return GCS_OK;
+}
+
+int32_t gcs_graph_builds(const gcs_ctx* c) { return c ? c->graph_builds : 0; }
 
 int gcs_step_host(gcs_ctx* c, const gcs_params* p, Star* host) {
     if (!c || !host) return GCS_ERR_ARG;
@@ -559,7 +758,7 @@ int gcs_device_status(gcs_ctx* c, uint32_t* status, int32_t clear) {
     cudaSetDevice(c->device);
     GCS_CUDA(c, cudaStreamSynchronize(c->stream));
     GCS_CUDA(c, cudaMemcpy(status, c->status, sizeof(uint32_t), cudaMemcpyDeviceToHost));
-    if (clear) GCS_CUDA(c, cudaMemset(c->status, 0, sizeof(uint32_t)));
+    if (clear) GCS_CUDA(c, cudaMemsetAsync(c->status, 0, sizeof(uint32_t), c->stream));
     return GCS_OK;
 }
 
@@ -650,7 +849,7 @@ int gcs_autotune(gcs_ctx* c, gcs_params* p, double* best_walk_ms) {
         rc = gcs_set_group_width(c, gw);
         if (rc) break;
         for (int L : leaves) {
-            if (L > p->leaf_size) continue;
+            if (L > p->leaf_size || L < p->tune_leaf_min) continue;
             for (int b : batches) {
                 for (int occ : occupancy) {
                     gcs_params q = *p;

@@ -66,6 +66,8 @@ struct ScratchLayout {
 };
 
 // ---- launchers (one per stage; all asynchronous on `st`) ----------------
+void launch_fill_segment_ids(const int64_t* seg_off, int nseg, int32_t* seg_id, int64_t n,
+                             cudaStream_t st);
 void launch_unpack_stars(const Star* stars, float4* pos, float4* vel, int64_t n, cudaStream_t st);
 void launch_pack_stars(const float4* pos, const float4* vel, Star* out, int64_t n, cudaStream_t st);
 void launch_pack_playback(const float4* pos, const float4* vel, PlaybackStar* out, int64_t n,

@@ -28,6 +28,22 @@ int stream_grid(int64_t n) {
     return (int)want;
 }
 
+// seg_id[i] = the segment s with seg_off[s] <= i < seg_off[s+1] (binary
+// search over the nseg+1 offsets, which stay in L1).
+__global__ void fill_segment_ids_kernel(const int64_t* __restrict__ seg_off, int nseg,
+                                        int32_t* __restrict__ seg_id, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        int lo = 0, hi = nseg - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(seg_off + mid) <= i) lo = mid;
+            else hi = mid - 1;
+        }
+        seg_id[i] = lo;
+    }
+}
+
 // Star (x,y,z,vx | vy,vz,m,tcol) <-> pos (x,y,z,m), vel (vx,vy,vz,tcol).
 __global__ void unpack_stars_kernel(const float4* __restrict__ stars, float4* __restrict__ pos,
                                     float4* __restrict__ vel, int64_t n) {
@@ -280,6 +296,12 @@ __global__ void direct_fp64_kernel(const float4* __restrict__ pos, int64_t seg_f
 }
 
 }  // namespace
+
+void launch_fill_segment_ids(const int64_t* seg_off, int nseg, int32_t* seg_id, int64_t n,
+                             cudaStream_t st) {
+    if (n <= 0) return;
+    fill_segment_ids_kernel<<<stream_grid(n), kStreamThreads, 0, st>>>(seg_off, nseg, seg_id, n);
+}
 
 void launch_unpack_stars(const Star* stars, float4* pos, float4* vel, int64_t n, cudaStream_t st) {
     if (n <= 0) return;

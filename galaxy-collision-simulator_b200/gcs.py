@@ -43,7 +43,7 @@ class Params(C.Structure):
                 ("leaf_size", C.c_int32), ("bounds_mode", C.c_int32), ("global_min", C.c_float),
                 ("global_max", C.c_float), ("recolor", C.c_int32), ("com_fp64", C.c_int32),
                 ("walk_batch", C.c_int32), ("walk_blocks_per_sm", C.c_int32),
-                ("with_potential", C.c_int32), ("reserved", C.c_int32 * 3)]
+                ("with_potential", C.c_int32), ("tune_leaf_min", C.c_int32), ("reserved", C.c_int32 * 2)]
 
 
 class GalaxySpec(C.Structure):
@@ -58,6 +58,11 @@ class GalaxySpec(C.Structure):
 class CollisionSpec(C.Structure):
     _fields_ = [("galaxy", GalaxySpec * 2), ("seed", C.c_uint64), ("G", C.c_float),
                 ("disc_dispersion", C.c_float)]
+
+
+class ServerResult(C.Structure):
+    _fields_ = [("id", C.c_uint64), ("n", C.c_int64), ("steps", C.c_int32), ("status", C.c_int32),
+                ("queued_ms", C.c_double), ("latency_ms", C.c_double)]
 
 
 class GcsError(RuntimeError):
@@ -112,6 +117,22 @@ def lib() -> C.CDLL:
         "gcs_set_group_width": (C.c_int, [P, i32]),
         "gcs_group_width": (i32, [P]),
         "gcs_sort_pairs_static": (C.c_int, [P, P, P, P, i64, P, P]),
+        "gcs_set_graphs": (C.c_int, [P, i32]),
+        "gcs_graph_builds": (i32, [P]),
+        "gcs_relayout": (C.c_int, [P, i32, C.POINTER(i64), C.POINTER(i32)]),
+        "gcs_segment_offset": (i64, [P, i32]),
+        "gcs_device_bytes": (i64, [P]),
+        "gcs_context_bytes": (i64, [i64, i32, i32]),
+        "gcs_server_create": (C.c_int, [C.POINTER(P), i32, i64, i32, C.c_double, C.POINTER(Params)]),
+        "gcs_server_destroy": (None, [P]),
+        "gcs_server_context": (P, [P]),
+        "gcs_server_capacity": (i64, [P]),
+        "gcs_server_last_error": (C.c_char_p, [P]),
+        "gcs_server_set_output": (C.c_int, [P, C.c_char_p, i32]),
+        "gcs_server_submit": (C.c_int, [P, u64, P, i64, i32]),
+        "gcs_server_tick": (C.c_int, [P, C.POINTER(i64)]),
+        "gcs_server_counts": (C.c_int, [P, C.POINTER(i64)]),
+        "gcs_server_pop": (C.c_int, [P, C.POINTER(ServerResult), P, i64]),
         "gcs_dropin_set_params": (C.c_int, [C.POINTER(Params)]),
         "gcs_dropin_context": (P, []),
         "gcs_dropin_device_stars": (P, []),
@@ -215,6 +236,21 @@ class Context:
         arr = (C.c_int64 * len(counts))(*[int(c) for c in counts])
         self.check(self.L.gcs_set_segments(self._h, len(counts), arr))
 
+    def relayout(self, counts, src_segments) -> None:
+        """New layout keeping the device state of segments src_segments[s] >= 0."""
+        k = len(counts)
+        assert len(src_segments) == k
+        c = (C.c_int64 * k)(*[int(x) for x in counts])
+        src = (C.c_int32 * k)(*[int(x) for x in src_segments])
+        self.check(self.L.gcs_relayout(self._h, k, c, src))
+
+    def segment_offset(self, segment: int) -> int:
+        return int(self.L.gcs_segment_offset(self._h, segment))
+
+    @property
+    def device_bytes(self) -> int:
+        return int(self.L.gcs_device_bytes(self._h))
+
     @property
     def n(self) -> int:
         return int(self.L.gcs_num_particles(self._h))
@@ -292,6 +328,13 @@ class Context:
         self.check(self.L.gcs_autotune(self._h, C.byref(q), C.byref(ms)))
         return q, ms.value
 
+    def set_graphs(self, enable: bool) -> None:
+        self.check(self.L.gcs_set_graphs(self._h, int(enable)))
+
+    @property
+    def graph_builds(self) -> int:
+        return int(self.L.gcs_graph_builds(self._h))
+
     @property
     def group_width(self) -> int:
         return int(self.L.gcs_group_width(self._h))
@@ -339,3 +382,101 @@ def stars_from_pos_vel(pos: np.ndarray, vel: np.ndarray) -> np.ndarray:
     out["g"] = (tcol >> 16) & 0xFF
     out["b"] = (tcol >> 24) & 0xFF
     return out
+
+
+class Server:
+    """Continuous batching of collision scenarios (gcs_server_*)."""
+
+    def __init__(self, p: Params, max_particles: int, max_segments: int, hbm_budget_bytes: float,
+                 device: int = 0):
+        self.L = lib()
+        self._h = C.c_void_p()
+        rc = self.L.gcs_server_create(C.byref(self._h), device, max_particles, max_segments,
+                                      float(hbm_budget_bytes), C.byref(p))
+        if rc != OK:
+            raise GcsError("gcs_server_create failed: %s" % self.L.gcs_status_string(rc).decode())
+        self._sizes = {}
+
+    def close(self) -> None:
+        if self._h:
+            self.L.gcs_server_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def check(self, rc: int) -> None:
+        if rc != OK:
+            msg = self.L.gcs_status_string(rc).decode()
+            raise GcsError("gcs server call failed (%d): %s: %s" % (
+                rc, msg, (self.L.gcs_server_last_error(self._h) or b"").decode()))
+
+    @property
+    def capacity(self) -> int:
+        return int(self.L.gcs_server_capacity(self._h))
+
+    @property
+    def device_bytes(self) -> int:
+        return int(self.L.gcs_device_bytes(self.L.gcs_server_context(self._h)))
+
+    def set_output(self, directory: str | None, frame_every: int = 0) -> None:
+        d = directory.encode() if directory else None
+        self.check(self.L.gcs_server_set_output(self._h, d, frame_every))
+
+    def submit(self, sid: int, stars: np.ndarray, steps: int) -> None:
+        stars = np.ascontiguousarray(stars, dtype=STAR_DTYPE)
+        self.check(self.L.gcs_server_submit(self._h, sid, _ptr(stars), len(stars), steps))
+        self._sizes[sid] = len(stars)
+
+    def tick(self) -> tuple:
+        out = (C.c_int64 * 4)()
+        self.check(self.L.gcs_server_tick(self._h, out))
+        return tuple(int(x) for x in out)
+
+    def counts(self) -> tuple:
+        out = (C.c_int64 * 3)()
+        self.check(self.L.gcs_server_counts(self._h, out))
+        return tuple(int(x) for x in out)
+
+    def pop(self, with_stars: bool = True):
+        """(ServerResult, Stars or None), or None if nothing has finished."""
+        info = ServerResult()
+        buf = None
+        cap = 0
+        ptr = None
+        if with_stars:
+            cap = max(self._sizes.values()) if self._sizes else 0
+            buf = np.zeros(cap, dtype=STAR_DTYPE)
+            ptr = _ptr(buf)
+        rc = self.L.gcs_server_pop(self._h, C.byref(info), ptr, cap)
+        if rc == 0:
+            return None
+        if rc < 0:
+            self.check(rc)
+        self._sizes.pop(int(info.id), None)
+        return info, (buf[:info.n].copy() if with_stars else None)
+
+
+def context_bytes(capacity: int, max_segments: int = 1, device: int = 0) -> int:
+    """Device bytes a Context(capacity, max_segments) would hold."""
+    b = int(lib().gcs_context_bytes(capacity, max_segments, device))
+    if b < 0:
+        _check(b, None)
+    return b
+
+
+def read_playback(path: str, n: int) -> np.ndarray:
+    """Frames of a simulation.bin-format file as an array [frames, n] of PlaybackStar."""
+    raw = np.fromfile(path, dtype=PLAYBACK_DTYPE)
+    if len(raw) % n:
+        raise GcsError("%s holds %d records, not a whole number of %d-star frames" % (path, len(raw), n))
+    return raw.reshape(-1, n)

@@ -71,7 +71,8 @@ typedef struct gcs_params {
     int32_t walk_batch; /* nodes fetched per stack pop, 1..64 (0 = default 32) */
     int32_t walk_blocks_per_sm; /* persistent walk occupancy (0 = default) */
     int32_t with_potential; /* 1: the walk also sums potentials (ACCEL .w) */
-    int32_t reserved[3];
+    int32_t tune_leaf_min;  /* gcs_autotune: smallest leaf size it may pick (0 = 1) */
+    int32_t reserved[2];
 } gcs_params;
 
 /* The reference's fixed settings: G=1, eps^2=10, theta=1, dt=0.01, L=1,
@@ -100,6 +101,13 @@ const char* gcs_last_error(const gcs_ctx* ctx);
  * particles [off_s, off_s + counts[s]).  Changing the layout invalidates the
  * particle data. */
 int gcs_set_segments(gcs_ctx* ctx, int32_t num_segments, const int64_t* counts);
+/* Change the layout keeping the particles of some segments: new segment s
+ * takes over old segment src_segment[s] (same count) or, with -1, starts
+ * empty (upload its Stars afterwards at gcs_segment_offset).  Kept segments
+ * are copied on the device; their state is unchanged. */
+int gcs_relayout(gcs_ctx* ctx, int32_t num_segments, const int64_t* counts, const int32_t* src_segment);
+/* First particle of `segment` (segment == number of segments gives N). */
+int64_t gcs_segment_offset(const gcs_ctx* ctx, int32_t segment);
 int64_t gcs_num_particles(const gcs_ctx* ctx);
 int32_t gcs_num_segments(const gcs_ctx* ctx);
 
@@ -122,6 +130,13 @@ int gcs_download_playback(gcs_ctx* ctx, PlaybackStar* host, int64_t offset, int6
 /* ---- stepping ----------------------------------------------------------- */
 /* One full step of every segment, queued on the context stream. */
 int gcs_step(gcs_ctx* ctx, const gcs_params* p);
+/* With graphs on, gcs_step launches the whole step as one CUDA graph
+ * (captured on first use, one graph per ping-pong parity of the particle
+ * arrays) and recaptures only when the parameters, the segment layout, the
+ * group width or the stream change.  Needs a non-default stream. */
+int gcs_set_graphs(gcs_ctx* ctx, int32_t enable);
+/* How many times the step graphs have been captured on this context. */
+int32_t gcs_graph_builds(const gcs_ctx* ctx);
 /* One step, then pack every particle as Star into `host` (pinned for an
  * asynchronous-capable copy) and synchronise: the reference's
  * cuda_physics_step with use_interop=false (cuda_engine.cu:379-451). */
@@ -232,7 +247,9 @@ int gcs_diagnostics(gcs_ctx* ctx, int32_t segment, double out[6]);
  * evaluations accepted by every active lane}. */
 int gcs_count_interactions(gcs_ctx* ctx, const gcs_params* p, uint64_t out[8]);
 /* Autotuner: times the walk on the current state for leaf sizes
- * {1,2,4,8,16,32} up to p->leaf_size (the caller's "leaf <= L"), pop
+ * {1,2,4,8,16,32} from p->tune_leaf_min up to p->leaf_size (the caller's
+ * "leaf <= L"; leaf size 2 gives exactly the reference's terms, sizes >= 3
+ * replace monopoles inside small opened nodes by exact sums), pop
  * batches {16,32,64}, group widths {32,16} and two occupancies, then writes the
  * fastest leaf_size / walk_batch / walk_blocks_per_sm into *p and keeps the
  * fastest group width on the context.  It runs bounds..aggregate once (the
@@ -263,6 +280,59 @@ int gcs_sort_pairs_static(uint64_t* keys, uint32_t* vals, uint64_t* keys_alt, ui
  * Reads the current positions; eps^2 and G from p. */
 int gcs_direct_accels_fp64(gcs_ctx* ctx, const gcs_params* p, int32_t segment,
                            const int64_t* targets, int64_t n_targets, double* out);
+/* Device bytes the context holds. */
+int64_t gcs_device_bytes(const gcs_ctx* ctx);
+/* Device bytes gcs_create(capacity, max_segments, device) would allocate
+ * (nothing is allocated); a negative status on bad arguments or device. */
+int64_t gcs_context_bytes(int64_t capacity, int32_t max_segments, int32_t device);
+
+/* ---- serving ---------------------------------------------------------------
+ * Continuous batching of independent collision scenarios on one device (no
+ * counterpart in the reference, whose engine holds one simulation in
+ * file-scope globals, cuda_engine.cu:16-44).  Requests are queued by
+ * gcs_server_submit; every gcs_server_tick admits queued scenarios in
+ * arrival order while segment slots and particle capacity allow, lays the
+ * resident scenarios out as segments of one context (kept scenarios stay
+ * on the device; the step graph is captured again only after a membership
+ * change), advances all of them by one step with one launch per stage, and
+ * retires those that reached their step count.  Each scenario's final
+ * Stars are byte-identical to stepping it alone with the same parameters.
+ * Not thread-safe: one host thread drives a server. */
+typedef struct gcs_server gcs_server;
+typedef struct gcs_server_result {
+    uint64_t id;
+    int64_t n;
+    int32_t steps;
+    int32_t status;    /* GCS_OK, or GCS_ERR_DEVICE if a status bit was raised */
+    double queued_ms;  /* submit -> admission */
+    double latency_ms; /* submit -> final Stars on the host */
+} gcs_server_result;
+/* A server on `device` holding up to max_segments scenarios and
+ * max_particles particles, shrunk so that its whole device footprint stays
+ * within hbm_budget_bytes (gcs_server_capacity gives the result). */
+int gcs_server_create(gcs_server** out, int32_t device, int64_t max_particles,
+                      int32_t max_segments, double hbm_budget_bytes, const gcs_params* p);
+void gcs_server_destroy(gcs_server* srv);
+/* The context underneath (for diagnostics; do not change its layout). */
+gcs_ctx* gcs_server_context(gcs_server* srv);
+int64_t gcs_server_capacity(const gcs_server* srv);
+const char* gcs_server_last_error(const gcs_server* srv);
+/* With dir set, scenario <id> writes <dir>/<id>.bin in the simulation.bin
+ * format (frames of n PlaybackStar records, main.cpp:264-272): a frame every
+ * frame_every steps (0: none) and always its final frame. */
+int gcs_server_set_output(gcs_server* srv, const char* dir, int32_t frame_every);
+/* Queue a scenario (Stars are copied); GCS_ERR_CAPACITY if n exceeds the
+ * server's particle capacity. */
+int gcs_server_submit(gcs_server* srv, uint64_t id, const Star* stars, int64_t n, int32_t steps);
+/* One scheduling round; out (may be NULL) = {resident scenarios, resident
+ * particles, admitted this round, retired this round}.  At most two steps
+ * are in flight on the device when it returns. */
+int gcs_server_tick(gcs_server* srv, int64_t out[4]);
+/* out = {queued, resident, finished and not yet popped}. */
+int gcs_server_counts(const gcs_server* srv, int64_t out[3]);
+/* Pop the oldest finished scenario: returns 1 and fills info (and host, if
+ * not NULL, with its n final Stars), 0 if none has finished. */
+int gcs_server_pop(gcs_server* srv, gcs_server_result* info, Star* host, int64_t host_capacity);
 
 #ifdef __cplusplus
 }

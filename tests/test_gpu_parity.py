@@ -177,6 +177,35 @@ def test_group_width_and_autotune(gcs_mod, oracle_mod, stars):
         assert ctx.device_status() == 0
 
 
+def test_graph_steps_match_eager_steps(gcs_mod, stars):
+    """The captured step is the eager step: byte-identical state after
+    several steps, one capture per parameter set."""
+    import torch
+    gcs = gcs_mod
+    s = torch.cuda.Stream()
+    with _ctx(gcs, stars) as eager, _ctx(gcs, stars) as graph:
+        eager.set_stream(s.cuda_stream)
+        graph.set_stream(s.cuda_stream)
+        graph.set_graphs(True)
+        p = _params(gcs, leaf_size=4, com_fp64=1)
+        for _ in range(5):
+            eager.step(p)
+            graph.step(p)
+        assert graph.graph_builds == 1
+        assert eager.download().tobytes() == graph.download().tobytes()
+        q = _params(gcs, leaf_size=8, com_fp64=1)
+        for _ in range(3):
+            eager.step(q)
+            graph.step(q)
+        assert graph.graph_builds == 2
+        assert eager.download().tobytes() == graph.download().tobytes()
+        np.testing.assert_array_equal(eager.read(gcs.BUF_ACCEL), graph.read(gcs.BUF_ACCEL))
+        assert graph.device_status() == 0
+    with _ctx(gcs, stars) as c:
+        with pytest.raises(gcs.GcsError):  # the legacy default stream cannot be captured
+            c.set_graphs(True)
+
+
 def test_integrate_bitexact(gcs_mod, oracle_mod, stars):
     gcs = gcs_mod
     with _ctx(gcs, stars) as ctx:
