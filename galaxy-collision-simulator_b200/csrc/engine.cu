@@ -803,12 +803,16 @@ int gcs_read_buffer(gcs_ctx* c, int32_t which, void* host, int64_t first, int64_
 }
 
 int gcs_diagnostics(gcs_ctx* c, int32_t segment, double out[6]) {
+    return gcs_diagnostics_kicked(c, segment, 0.0, out);
+}
+
+int gcs_diagnostics_kicked(gcs_ctx* c, int32_t segment, double kick, double out[6]) {
     if (!c || !out || segment < 0 || segment >= c->nseg) return GCS_ERR_ARG;
     cudaSetDevice(c->device);
     const int64_t first = c->h_seg_off[segment];
     const int64_t n = c->h_seg_off[segment + 1] - first;
     GCS_CUDA(c, cudaMemsetAsync(c->diag, 0, sizeof(double) * 6, c->stream));
-    launch_diag(c->pos[c->cur], c->vel[c->cur], c->acc, first, n, c->diag, c->stream);
+    launch_diag(c->pos[c->cur], c->vel[c->cur], c->acc, first, n, kick, c->diag, c->stream);
     int rc = check_launch(c, "diag");
     if (rc) return rc;
     GCS_CUDA(c, cudaMemcpyAsync(out, c->diag, sizeof(double) * 6, cudaMemcpyDeviceToHost, c->stream));

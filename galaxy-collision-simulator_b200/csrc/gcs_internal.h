@@ -121,7 +121,7 @@ void launch_integrate(float4* pos, float4* vel, const float4* acc, float dt, int
 void launch_kick(float4* vel, const float4* acc, float dt, int64_t n, cudaStream_t st);
 
 void launch_diag(const float4* pos, const float4* vel, const float4* acc, int64_t first, int64_t n,
-                 double* out6, cudaStream_t st);
+                 double kick, double* out6, cudaStream_t st);
 // Pack the context's current particles as Star[] into a device buffer and
 // wait for it (the headless interop target of the drop-in API).
 int pack_to_device(gcs_ctx* c, Star* dst);

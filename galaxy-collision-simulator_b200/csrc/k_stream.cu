@@ -224,21 +224,27 @@ __global__ void kick_kernel(float4* __restrict__ vel, const float4* __restrict__
 // [first, first+n).  out = {KE, px, py, pz, M, PE}; PE = 0.5 sum m phi with
 // phi from the walk's potential lane (acc.w).  Blocks reduce in shared
 // memory and add with FP64 atomics.
+// Velocities enter as v + a * kick (in FP64): kick = dt/2 turns the stored
+// half-step velocities of the leapfrog into synchronised ones.
 __global__ void diag_kernel(const float4* __restrict__ pos, const float4* __restrict__ vel,
-                            const float4* __restrict__ accp, int64_t first, int64_t n,
+                            const float4* __restrict__ accp, int64_t first, int64_t n, double kick,
                             double* __restrict__ out) {
     double acc[6] = {0, 0, 0, 0, 0, 0};
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
         const float4 p = __ldg(pos + first + i);
         const float4 v = __ldg(vel + first + i);
+        const float4 a = __ldg(accp + first + i);
         const double m = p.w;
-        acc[0] += 0.5 * m * ((double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z);
-        acc[1] += m * v.x;
-        acc[2] += m * v.y;
-        acc[3] += m * v.z;
+        const double vx = (double)v.x + (double)a.x * kick;
+        const double vy = (double)v.y + (double)a.y * kick;
+        const double vz = (double)v.z + (double)a.z * kick;
+        acc[0] += 0.5 * m * (vx * vx + vy * vy + vz * vz);
+        acc[1] += m * vx;
+        acc[2] += m * vy;
+        acc[3] += m * vz;
         acc[4] += m;
-        acc[5] += 0.5 * m * (double)__ldg(accp + first + i).w;
+        acc[5] += 0.5 * m * (double)a.w;
     }
     __shared__ double s[6][kStreamThreads / 32];
     for (int k = 0; k < 6; ++k) {
@@ -362,9 +368,9 @@ void launch_kick(float4* vel, const float4* acc, float dt, int64_t n, cudaStream
 }
 
 void launch_diag(const float4* pos, const float4* vel, const float4* acc, int64_t first, int64_t n,
-                 double* out6, cudaStream_t st) {
+                 double kick, double* out6, cudaStream_t st) {
     if (n <= 0) return;
-    diag_kernel<<<stream_grid(n), kStreamThreads, 0, st>>>(pos, vel, acc, first, n, out6);
+    diag_kernel<<<stream_grid(n), kStreamThreads, 0, st>>>(pos, vel, acc, first, n, kick, out6);
 }
 
 void launch_direct_fp64(const float4* pos, int64_t seg_first, int64_t seg_n, const int64_t* targets,

@@ -110,6 +110,7 @@ def lib() -> C.CDLL:
         "gcs_collision_count": (i64, [C.POINTER(CollisionSpec)]),
         "gcs_generate_collision": (C.c_int, [C.POINTER(CollisionSpec), P, i64]),
         "gcs_diagnostics": (C.c_int, [P, i32, C.POINTER(C.c_double)]),
+        "gcs_diagnostics_kicked": (C.c_int, [P, i32, C.c_double, C.POINTER(C.c_double)]),
         "gcs_direct_accels_fp64": (C.c_int, [P, C.POINTER(Params), i32, C.POINTER(i64), i64,
                                              C.POINTER(C.c_double)]),
         "gcs_count_interactions": (C.c_int, [P, C.POINTER(Params), C.POINTER(C.c_uint64)]),
@@ -314,9 +315,10 @@ class Context:
         self.check(self.L.gcs_read_buffer(self._h, which, _ptr(out), first, count))
         return out
 
-    def diagnostics(self, segment: int = 0) -> np.ndarray:
+    def diagnostics(self, segment: int = 0, kick: float = 0.0) -> np.ndarray:
+        """{KE, px, py, pz, M, PE} in FP64; velocities taken as v + a * kick."""
         out = (C.c_double * 6)()
-        self.check(self.L.gcs_diagnostics(self._h, segment, out))
+        self.check(self.L.gcs_diagnostics_kicked(self._h, segment, kick, out))
         return np.array(out[:])
 
     def autotune(self, p: Params) -> tuple[Params, float]:

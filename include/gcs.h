@@ -237,6 +237,11 @@ int gcs_generate_collision(const gcs_collision_spec* spec, Star* out, int64_t n)
  * 0.5 * sum m_i phi_i over the potentials of the last walk, which must have
  * run with with_potential = 1 at the current positions (else it is 0). */
 int gcs_diagnostics(gcs_ctx* ctx, int32_t segment, double out[6]);
+/* The same with every velocity taken as v + a * kick (FP64) from the last
+ * computed accelerations: after gcs_compute_accels at step n of the
+ * leapfrog (whose stored velocities are the half-step ones, v_{n-1/2}),
+ * kick = dt/2 gives the energy and momentum at the synchronised v_n. */
+int gcs_diagnostics_kicked(gcs_ctx* ctx, int32_t segment, double kick, double out[6]);
 /* Interaction counts of one walk at the current state: runs bounds..walk
  * with the counting walk and returns {monopole terms, particle terms}
  * summed over all targets (the unit of interactions/s; 20 FP32 flops each),
