@@ -63,6 +63,12 @@ __device__ __forceinline__ float rsqrt_approx(float x) {
     return r;
 }
 
+// Two softened distances at once (sm_100 packed FP32): each element is
+// rounded exactly as softened_d2 rounds it.
+__device__ __forceinline__ float2 softened_d2_x2(float2 dx, float2 dy, float2 dz, float2 eps2) {
+    return __fadd2_rn(__ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx))), eps2);
+}
+
 // ---- opening criterion (cuda_engine.cu:143 with theta) ---------------------
 // A node is used as a monopole iff width^2 < theta^2 * d2 (d2 softened).
 // width^2 is formed once per node when it is staged.

@@ -75,19 +75,42 @@ constexpr int kClassMixed = 3;  // lanes decide one by one
 constexpr float kBoxLo = 1.0f - 1.0f / 65536.0f;
 constexpr float kBoxHi = 1.0f + 1.0f / 65536.0f;
 
-// Per-warp shared memory for H nodes per lane per round.
+// Per-warp shared memory for H nodes per lane per round.  Nodes and sources
+// to evaluate are stored in pairs (slot 2q and 2q+1 side by side), so that
+// one packed FP32 instruction (sm_100 f32x2) evaluates two of them: take
+// nodes fill slots [0, n_take), mixed nodes start at the next even slot, and
+// an odd list is padded with an empty entry (mass 0 at 1e30 in every
+// coordinate, lane mask 0).
 template <int H>
 struct WarpSmem {
     static constexpr int kBatch = 32 * H;
+    static constexpr int kPairs = kBatch / 2 + 1;                  // two padded lists
     static constexpr int kStackCap = 256 + 64 * H;                 // stack entries
     static constexpr int kSpillAbove = kStackCap - 2 * kBatch;     // a round pushes <= 2*batch
     int2 stk[kStackCap];          // node, lane mask
-    float4 nc[kBatch];            // com x, y, z, G*mass (compacted: take, then mixed)
-    uint2 nw[kBatch];             // bits of width^2, lane mask
-    uint32_t nopen[kBatch];       // opening lanes of each mixed node
-    float4 src[kSrcCap];          // x, y, z, G*mass
-    int2 srcm[kSrcCap];           // particle, lane mask
+    float4 pxy[kPairs];           // x0 x1 y0 y1 of the centres of mass of slots 2q, 2q+1
+    float4 pzm[kPairs];           // z0 z1 Gm0 Gm1
+    float2 pw2[kPairs];           // width^2 of both slots
+    uint2 pmask[kPairs];          // lane masks of both slots
+    uint2 pnopen[kPairs];         // opening lanes of both slots (mixed nodes)
+    float4 sxy[kSrcCap / 2];      // particle sources in pairs: x0 x1 y0 y1
+    float4 szm[kSrcCap / 2];      // z0 z1 Gm0 Gm1
+    uint2 smask[kSrcCap / 2];     // lane masks
+    int2 srcm[kSrcCap];           // particle, lane mask (the list before its fetch)
 };
+
+// Store one evaluation entry at pair slot `slot` of a pair-interleaved list.
+__device__ __forceinline__ void put_pair(float4* xy, float4* zm, uint2* mk, int slot, float4 c,
+                                         uint32_t mask) {
+    const int q = slot >> 1, e = slot & 1;
+    float* fxy = reinterpret_cast<float*>(xy + q);
+    float* fzm = reinterpret_cast<float*>(zm + q);
+    fxy[e] = c.x;
+    fxy[2 + e] = c.y;
+    fzm[e] = c.z;
+    fzm[2 + e] = c.w;
+    reinterpret_cast<uint32_t*>(mk + q)[e] = mask;
+}
 
 // Resident blocks per SM the register budget is set for (H=1: 48 registers
 // a thread, 40 warps; H=2: 64 registers, 32 warps).
@@ -97,7 +120,7 @@ struct WalkOcc {
 };
 
 struct Accum {
-    float ax, ay, az, pot;
+    float2 ax, ay, az, pot;       // two partial sums per component (even / odd slots)
     uint32_t n_mono, n_part;      // interaction counts (count mode only)
     uint32_t w_node, w_src;       // warp-wide node / source evaluations (count mode only)
     uint32_t rounds, spills;      // pop rounds, stack spills to global memory
@@ -106,34 +129,102 @@ struct Accum {
 
 // Sum the listed particle sources into every lane whose bit is in the
 // source's mask (leaf rule: skip d2 <= 1.01 eps^2).
+// Two evaluation entries for this lane, packed (sm_100 f32x2): d = c - x and
+// the softened d2 of both, then the terms of the entries whose `use` is
+// set.  Each element is rounded exactly as the scalar forms round it
+// (softened_d2, the hardware 1/sqrt, inv^3, G m inv^3, one FMA per
+// component); each lane keeps two partial sums (even and odd slots).
+struct PairD {
+    float2 dx, dy, dz, d2;
+};
+
+__device__ __forceinline__ PairD pair_d(float4 xy, float4 zm, float2 npx, float2 npy, float2 npz, float2 e2) {
+    PairD r;
+    r.dx = __fadd2_rn(make_float2(xy.x, xy.y), npx);
+    r.dy = __fadd2_rn(make_float2(xy.z, xy.w), npy);
+    r.dz = __fadd2_rn(make_float2(zm.x, zm.y), npz);
+    r.d2 = softened_d2_x2(r.dx, r.dy, r.dz, e2);
+    return r;
+}
+
+template <bool kPot>
+__device__ __forceinline__ void pair_add(Accum& A, const PairD& d, float4 zm, bool use0, bool use1) {
+    const float2 inv = make_float2(rsqrt_approx(d.d2.x), rsqrt_approx(d.d2.y));
+    const float2 inv3 = __fmul2_rn(__fmul2_rn(inv, inv), inv);
+    float2 f = __fmul2_rn(make_float2(zm.z, zm.w), inv3);
+    f.x = use0 ? f.x : 0.0f;
+    f.y = use1 ? f.y : 0.0f;
+    A.ax = __ffma2_rn(d.dx, f, A.ax);
+    A.ay = __ffma2_rn(d.dy, f, A.ay);
+    A.az = __ffma2_rn(d.dz, f, A.az);
+    if (kPot) {
+        const float2 t = __ffma2_rn(make_float2(-zm.z, -zm.w), inv, A.pot);
+        A.pot.x = use0 ? t.x : A.pot.x;
+        A.pot.y = use1 ? t.y : A.pot.y;
+    }
+}
+
+// Sum the listed particle sources into every lane whose bit is in the
+// source's mask (leaf rule: skip d2 <= 1.01 eps^2).
+// One packed evaluation of two entries for this lane: terms of the entries
+// whose `use` is set are added to the two partial sums.  Each term is
+// rounded exactly as the scalar form (d = c - x, softened_d2, the hardware
+// 1/sqrt, inv^3, G m inv^3, one FMA per component).
+template <bool kPot>
+__device__ __forceinline__ void add_pair(Accum& A, float4 xy, float4 zm, float2 npx, float2 npy, float2 npz,
+                                         float2 e2, bool use0, bool use1, float2& d2_out, bool& d2_ready) {
+    (void)d2_ready;
+    const float2 dx = __fadd2_rn(make_float2(xy.x, xy.y), npx);
+    const float2 dy = __fadd2_rn(make_float2(xy.z, xy.w), npy);
+    const float2 dz = __fadd2_rn(make_float2(zm.x, zm.y), npz);
+    const float2 d2 = softened_d2_x2(dx, dy, dz, e2);
+    d2_out = d2;
+    const float2 inv = make_float2(rsqrt_approx(d2.x), rsqrt_approx(d2.y));
+    const float2 inv3 = __fmul2_rn(__fmul2_rn(inv, inv), inv);
+    float2 f = __fmul2_rn(make_float2(zm.z, zm.w), inv3);
+    f.x = use0 ? f.x : 0.0f;
+    f.y = use1 ? f.y : 0.0f;
+    A.ax = __ffma2_rn(dx, f, A.ax);
+    A.ay = __ffma2_rn(dy, f, A.ay);
+    A.az = __ffma2_rn(dz, f, A.az);
+    if (kPot) {
+        const float2 t = __ffma2_rn(make_float2(-zm.z, -zm.w), inv, A.pot);
+        A.pot.x = use0 ? t.x : A.pot.x;
+        A.pot.y = use1 ? t.y : A.pot.y;
+    }
+}
+
+// Sum the listed particle sources into every lane whose bit is in the
+// source's mask (leaf rule: skip d2 <= 1.01 eps^2).
 template <int H, bool kPot, bool kCount>
 __device__ __forceinline__ void flush_sources(WarpSmem<H>& W, int nsrc, int lane, uint32_t lane_bit,
                                               const float4* __restrict__ pos, float G, float4 p,
                                               float eps2, float leaf_thr, Accum& A) {
     __syncwarp();
-    for (int e = lane; e < nsrc; e += 32) {
-        float4 q = __ldg(pos + W.srcm[e].x);
-        q.w = __fmul_rn(G, q.w);
-        W.src[e] = q;
+    const int padded = (nsrc + 1) & ~1;
+    for (int e = lane; e < padded; e += 32) {
+        float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+        uint32_t mask = 0u;
+        if (e < nsrc) {
+            const int2 sm = W.srcm[e];
+            q = __ldg(pos + sm.x);
+            q.w = __fmul_rn(G, q.w);
+            mask = (uint32_t)sm.y;
+        }
+        put_pair(W.sxy, W.szm, W.smask, e, q, mask);
     }
     __syncwarp();
-#pragma unroll 4
-    for (int e = 0; e < nsrc; ++e) {
-        const float4 q = W.src[e];
-        const uint32_t m = (uint32_t)W.srcm[e].y;
-        const float dx = __fsub_rn(q.x, p.x);
-        const float dy = __fsub_rn(q.y, p.y);
-        const float dz = __fsub_rn(q.z, p.z);
-        const float d2 = softened_d2(dx, dy, dz, eps2);
-        const bool use = (m & lane_bit) && (d2 > leaf_thr);
-        const float inv = rsqrt_approx(d2);
-        const float inv3 = __fmul_rn(__fmul_rn(inv, inv), inv);
-        const float f = use ? __fmul_rn(q.w, inv3) : 0.0f;
-        A.ax = __fmaf_rn(dx, f, A.ax);
-        A.ay = __fmaf_rn(dy, f, A.ay);
-        A.az = __fmaf_rn(dz, f, A.az);
-        if (kPot) A.pot = use ? __fmaf_rn(-q.w, inv, A.pot) : A.pot;
-        if (kCount) A.n_part += use ? 1u : 0u;
+    const float2 npx = make_float2(-p.x, -p.x), npy = make_float2(-p.y, -p.y), npz = make_float2(-p.z, -p.z);
+    const float2 e2 = make_float2(eps2, eps2);
+#pragma unroll 2
+    for (int q = 0; q < (padded >> 1); ++q) {
+        const float4 zm = W.szm[q];
+        const uint2 mk = W.smask[q];
+        const PairD d = pair_d(W.sxy[q], zm, npx, npy, npz, e2);
+        const bool use0 = (mk.x & lane_bit) && (d.d2.x > leaf_thr);
+        const bool use1 = (mk.y & lane_bit) && (d.d2.y > leaf_thr);
+        pair_add<kPot>(A, d, zm, use0, use1);
+        if (kCount) A.n_part += (use0 ? 1u : 0u) + (use1 ? 1u : 0u);
     }
     if (kCount) A.w_src += (uint32_t)nsrc;
     __syncwarp();
@@ -165,6 +256,7 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
     const uint32_t lane_bit = 1u << lane;
     const uint32_t lt = lane_bit - 1u;
     const float G = wp.G, eps2 = wp.eps2, theta2 = wp.theta2;
+    const float2 e2 = make_float2(eps2, eps2), th2 = make_float2(theta2, theta2);
     const float leaf_thr = __fmul_rn(eps2, 1.01f);
     const int leaf_size = wp.leaf_size;
     const int batch = wp.batch;
@@ -197,7 +289,10 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
         const int off = (int)__ldg(L.seg_off + s);
         const int seg_n = (int)__ldg(L.seg_off + s + 1) - off;
         const int seg_end = off + seg_n;
-        Accum A = {0.f, 0.f, 0.f, 0.f, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+        Accum A;
+        A.ax = A.ay = A.az = A.pot = make_float2(0.f, 0.f);
+        A.n_mono = A.n_part = A.w_node = A.w_src = A.rounds = A.spills = A.all_open = A.all_take = 0u;
+        const float2 npx = make_float2(-p.x, -p.x), npy = make_float2(-p.y, -p.y), npz = make_float2(-p.z, -p.z);
         int nsrc = 0;
 
         if (seg_n >= 2) {
@@ -297,19 +392,29 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                     n_take += __popc(bt[h]);
                     n_mixed += __popc(bm[h]);
                 }
+                // take nodes in slots [0, n_take), mixed nodes from the next
+                // even slot; odd lists are padded with an empty entry
+                const int mixed_base = (n_take + 1) & ~1;
                 int slot[H];
                 {
                     int take_before = 0, mixed_before = 0;
 #pragma unroll
                     for (int h = 0; h < H; ++h) {
                         slot[h] = cls[h] == kClassTake ? take_before + __popc(bt[h] & lt)
-                                : (cls[h] == kClassMixed ? n_take + mixed_before + __popc(bm[h] & lt) : -1);
+                                : (cls[h] == kClassMixed ? mixed_base + mixed_before + __popc(bm[h] & lt) : -1);
                         take_before += __popc(bt[h]);
                         mixed_before += __popc(bm[h]);
                         if (slot[h] >= 0) {
-                            W.nc[slot[h]] = com[h];
-                            W.nw[slot[h]] = make_uint2(__float_as_uint(w2[h]), my_mask[h]);
+                            put_pair(W.pxy, W.pzm, W.pmask, slot[h], com[h], my_mask[h]);
+                            reinterpret_cast<float*>(W.pw2 + (slot[h] >> 1))[slot[h] & 1] = w2[h];
                         }
+                    }
+                    const float4 empty = make_float4(1e30f, 1e30f, 1e30f, 0.0f);
+                    const int pad = lane == 0 ? ((n_take & 1) ? n_take : -1)
+                                  : lane == 1 ? ((n_mixed & 1) ? mixed_base + n_mixed : -1) : -1;
+                    if (pad >= 0) {
+                        put_pair(W.pxy, W.pzm, W.pmask, pad, empty, 0u);
+                        reinterpret_cast<float*>(W.pw2 + (pad >> 1))[1] = 0.0f;
                     }
                 }
                 __syncwarp();
@@ -319,46 +424,32 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                     A.all_open += (uint32_t)(b - n_take - n_mixed);
                     A.all_take += (uint32_t)n_take;
                 }
-                // 3a. nodes every lane accepts: monopole terms only
+                // 3a. nodes every lane accepts: monopole terms only, two
+                // nodes per packed evaluation
 #pragma unroll 2
-                for (int k = 0; k < n_take; ++k) {
-                    const float4 a = W.nc[k];
-                    const bool active = (W.nw[k].y & lane_bit) != 0u;
-                    const float dx = __fsub_rn(a.x, p.x);
-                    const float dy = __fsub_rn(a.y, p.y);
-                    const float dz = __fsub_rn(a.z, p.z);
-                    const float d2 = softened_d2(dx, dy, dz, eps2);
-                    const float inv = rsqrt_approx(d2);
-                    const float inv3 = __fmul_rn(__fmul_rn(inv, inv), inv);
-                    const float f = active ? __fmul_rn(a.w, inv3) : 0.0f;
-                    A.ax = __fmaf_rn(dx, f, A.ax);
-                    A.ay = __fmaf_rn(dy, f, A.ay);
-                    A.az = __fmaf_rn(dz, f, A.az);
-                    if (kPot) A.pot = active ? __fmaf_rn(-a.w, inv, A.pot) : A.pot;
-                    if (kCount) A.n_mono += active ? 1u : 0u;
+                for (int q = 0; q < ((n_take + 1) >> 1); ++q) {
+                    const float4 zm = W.pzm[q];
+                    const uint2 mk = W.pmask[q];
+                    const PairD d = pair_d(W.pxy[q], zm, npx, npy, npz, e2);
+                    const bool use0 = (mk.x & lane_bit) != 0u, use1 = (mk.y & lane_bit) != 0u;
+                    pair_add<kPot>(A, d, zm, use0, use1);
+                    if (kCount) A.n_mono += (use0 ? 1u : 0u) + (use1 ? 1u : 0u);
                 }
                 // 3b. mixed nodes: each lane's own test; lane 0 records the
-                // ballot of opening lanes for the node's owner
-                for (int k = n_take; k < n_take + n_mixed; ++k) {
-                    const float4 a = W.nc[k];
-                    const uint2 wm = W.nw[k];
-                    const bool active = (wm.y & lane_bit) != 0u;
-                    const float dx = __fsub_rn(a.x, p.x);
-                    const float dy = __fsub_rn(a.y, p.y);
-                    const float dz = __fsub_rn(a.z, p.z);
-                    const float d2 = softened_d2(dx, dy, dz, eps2);
-                    const bool take = accept_monopole(__uint_as_float(wm.x), d2, theta2);
-                    const bool mono = active && take;
-                    const float inv = rsqrt_approx(d2);
-                    const float inv3 = __fmul_rn(__fmul_rn(inv, inv), inv);
-                    const float f = mono ? __fmul_rn(a.w, inv3) : 0.0f;
-                    A.ax = __fmaf_rn(dx, f, A.ax);
-                    A.ay = __fmaf_rn(dy, f, A.ay);
-                    A.az = __fmaf_rn(dz, f, A.az);
-                    if (kPot) A.pot = mono ? __fmaf_rn(-a.w, inv, A.pot) : A.pot;
-                    if (kCount) A.n_mono += mono ? 1u : 0u;
-                    const uint32_t om = __ballot_sync(kFull, active && !take);
-                    if (lane == 0) W.nopen[k] = om;
+                // ballots of opening lanes for the nodes' owners
+                for (int q = mixed_base >> 1; q < ((mixed_base + n_mixed + 1) >> 1); ++q) {
+                    const float4 zm = W.pzm[q];
+                    const uint2 mk = W.pmask[q];
+                    const float2 w2q = W.pw2[q];
+                    const PairD d = pair_d(W.pxy[q], zm, npx, npy, npz, e2);
+                    const float2 lim = __fmul2_rn(d.d2, th2);  // accept_monopole: w^2 < d2 * theta^2
+                    const bool act0 = (mk.x & lane_bit) != 0u, act1 = (mk.y & lane_bit) != 0u;
+                    const bool take0 = w2q.x < lim.x, take1 = w2q.y < lim.y;
+                    pair_add<kPot>(A, d, zm, act0 && take0, act1 && take1);
+                    if (kCount) A.n_mono += (act0 && take0 ? 1u : 0u) + (act1 && take1 ? 1u : 0u);
+                    const uint32_t om0 = __ballot_sync(kFull, act0 && !take0);
+                    const uint32_t om1 = __ballot_sync(kFull, act1 && !take1);
+                    if (lane == 0) W.pnopen[q] = make_uint2(om0, om1);
                 }
                 __syncwarp();
                 // 4. parallel push / append for the opened nodes
@@ -368,7 +459,7 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
 #pragma unroll
                 for (int h = 0; h < H; ++h) {
                     my_open[h] = cls[h] == kClassOpen ? my_mask[h]
-                               : (cls[h] == kClassMixed ? W.nopen[slot[h]] : 0u);
+                               : (cls[h] == kClassMixed ? reinterpret_cast<const uint32_t*>(W.pnopen)[slot[h]] : 0u);
                     n_push[h] = 0;
                     n_src[h] = 0;
                     if (my_open[h] != 0u && code_b[h] != kSkipTag) {
@@ -457,7 +548,9 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
             }
         }
         if (nsrc > 0) flush_sources<H, kPot, kCount>(W, nsrc, lane, lane_bit, pos, G, p, eps2, leaf_thr, A);
-        if (valid) acc[t] = make_float4(A.ax, A.ay, A.az, A.pot);
+        if (valid)
+            acc[t] = make_float4(__fadd_rn(A.ax.x, A.ax.y), __fadd_rn(A.ay.x, A.ay.y), __fadd_rn(A.az.x, A.az.y),
+                                 __fadd_rn(A.pot.x, A.pot.y));
         if (kCount) {
             unsigned long long cm = A.n_mono, cp = A.n_part;
             for (int o = 16; o > 0; o >>= 1) {

@@ -5,7 +5,11 @@ Bars: bit-exact for keys, permutation, topology, bounds, masses, widths and
 the integrate step (same inputs); accelerations within 1e-5 relative
 (FP32 reassociation and rsqrtf vs IEEE 1/sqrt only), measured per particle
 as |a - a_ref| / max(|a_ref|, 1e-3 * median |a_ref|), required at the 99.9th
-percentile, with 1e-4 as the per-particle maximum."""
+percentile, with 1e-4 as the per-particle maximum.  At theta = 0 (a direct
+sum over every particle) the FP32 rounding of the sum itself, in any order,
+is above 1e-5 for the particles with the most cancellation; there the engine
+and the oracle are both compared with an FP64 direct sum and the engine must
+be at least as close as the oracle."""
 import ctypes as C
 
 import numpy as np
@@ -138,7 +142,20 @@ def test_walk_matches_oracle(gcs_mod, oracle_mod, stars, theta, leaf):
         nodes = ctx.read(gcs.BUF_NODES)
         acc = ctx.read(gcs.BUF_ACCEL)
         ref = oracle_mod.walk(sp, nodes, p.G, p.epsilon_sq, theta, leaf)
-        _assert_acc(acc[:, :3], ref[:, :3], "theta=%s L=%s" % (theta, leaf))
+        if theta > 0:
+            _assert_acc(acc[:, :3], ref[:, :3], "theta=%s L=%s" % (theta, leaf))
+        else:
+            # theta = 0 is a direct sum over every particle: its FP32 rounding
+            # (in the oracle's order or any other) exceeds 1e-5 for the
+            # particles with the most cancellation, so both sums are held to
+            # an FP64 direct sum and the engine must be at least as close
+            exact = ctx.direct_fp64(p, np.arange(len(sp)))
+            scale = np.median(np.linalg.norm(exact, axis=1))
+            e_gpu = rel_err(acc[:, :3], exact, floor=1e-3 * scale)
+            e_ref = rel_err(ref[:, :3], exact, floor=1e-3 * scale)
+            assert np.percentile(e_gpu, 99.9) <= max(TOL_ACC, np.percentile(e_ref, 99.9))
+            assert e_gpu.max() <= TOL_ACC_MAX
+            assert _acc_err(acc[:, :3], ref[:, :3]).max() <= TOL_ACC_MAX
         np.testing.assert_allclose(acc[:, 3], ref[:, 3], rtol=1e-5)
         assert ctx.device_status() == 0
 
