@@ -143,98 +143,160 @@ __device__ __forceinline__ ChildData load_child(int c, int n_internal, const flo
     return r;
 }
 
-__global__ void __launch_bounds__(256, 4)
+constexpr int kAggThreads = 256;
+
+// A node finished inside the block, kept in shared memory for its parent.
+struct LocalNode {
+    float3 lo, hi, com;
+    float m;
+    double3 mx;
+    double md;
+};
+
+__device__ __forceinline__ ChildData from_local(const LocalNode& q) {
+    ChildData r;
+    r.lo = q.lo;
+    r.hi = q.hi;
+    r.com = q.com;
+    r.m = q.m;
+    r.mx = q.mx;
+    r.md = q.md;
+    return r;
+}
+
+// One thread per particle; block b owns particles [256 b, 256 b + 256).  A
+// node whose particle range lies inside its block's range has both children
+// finished by threads of that block: its arrival counter and the finished
+// children live in shared memory and the handshake is block-scoped.  Every
+// other node uses the GPU-scope counter in its build record.  The side a
+// node uses depends only on the node, so both arrivals always meet.
+__global__ void __launch_bounds__(kAggThreads, 4)
 aggregate_kernel(Layout L, const float4* __restrict__ pos,
                                  BvhNodeTraverse* __restrict__ tr, BvhNodeBuild* __restrict__ bd,
                                  double4* __restrict__ com64, const int32_t* __restrict__ leaf_parent,
                                  int com_fp64, uint32_t* __restrict__ status) {
+    __shared__ int sflag[kAggThreads];
+    __shared__ LocalNode snode[kAggThreads];
     const bool fp64 = com_fp64 != 0;
-    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < L.n; g += gridDim.x * blockDim.x) {
-        // The node this thread has just finished (first the leaf itself) is
-        // carried in registers; at each parent only the sibling is loaded.
-        int from = L.n_internal + g;
-        ChildData mine = load_child(from, L.n_internal, pos, tr, bd, com64, fp64);
-        int node = __ldg(leaf_parent + g);
-        int levels = 0;
-        while (node >= 0) {
-            // a valid tree has at most 96 internal levels (strictly increasing
-            // prefix lengths below 96); more means malformed parent links
-            if (++levels > 96 || node >= L.n_internal) {
-                atomicOr(status, GCS_DEV_TREE_MALFORMED);
-                break;
-            }
-            // links come from the build launch: fetch them before the arrival
-            const int cl = __ldg(&tr[node].child_left);
-            const int cr = __ldg(&tr[node].child_right);
-            const int up = __ldg(&bd[node].parent);
+    const int b0 = blockIdx.x * kAggThreads;
+    sflag[threadIdx.x] = 0;
+    __syncthreads();
+    const int g = b0 + threadIdx.x;
+    if (g >= L.n) return;
+    const int s = L.nseg > 1 ? __ldg(L.seg_id + g) : 0;
+    // The node this thread has just finished (first the leaf itself) is
+    // carried in registers; at each parent only the sibling is loaded.
+    int from = L.n_internal + g;
+    ChildData mine = load_child(from, L.n_internal, pos, tr, bd, com64, fp64);
+    int node = __ldg(leaf_parent + g);
+    int levels = 0;
+    while (node >= 0) {
+        // a valid tree has at most 96 internal levels (strictly increasing
+        // prefix lengths below 96); more means malformed parent links
+        if (++levels > 96 || node >= L.n_internal) {
+            atomicOr(status, GCS_DEV_TREE_MALFORMED);
+            break;
+        }
+        // links come from the build launch: fetch them before the arrival
+        const int cl = __ldg(&tr[node].child_left);
+        const int cr = __ldg(&tr[node].child_right);
+        const int up = __ldg(&bd[node].parent);
+        const int re = __ldg(&tr[node].range_end);
+        const int own = node + s;  // particle index at this end of the node's range
+        const bool local = min(own, re) >= b0 && max(own, re) < b0 + kAggThreads;
+        int old;
+        if (local) {
+            // block scope: this thread's writes (shared and global) before
+            // the arrival, the sibling's after it
+            __threadfence_block();
+            old = atomicAdd(&sflag[own - b0], 1);
+            if (old == 0) break;
+            __threadfence_block();
+        } else if (levels == 1) {
+            // At the leaf level this thread has written nothing, so its
+            // arrival needs no release; it acquires only if it arrives second.
+            old = arrive_relaxed(&bd[node].flag);
+            if (old == 0) break;
+            fence_acq_rel();
+        } else {
             // release: this thread's writes of the child it just finished are
             // visible to whoever acquires the counter next; acquire: the
             // second arrival sees the sibling's writes
-            // At the leaf level this thread has written nothing, so its
-            // arrival needs no release; it acquires only if it arrives second.
-            int old;
-            if (levels == 1) {
-                old = arrive_relaxed(&bd[node].flag);
-                if (old != 0) fence_acq_rel();
-            } else {
-                old = arrive_acq_rel(&bd[node].flag);
-            }
-            if (old == 0) break;                    // first arrival: the sibling finishes
-            if (cl < 0 || cr < 0 || cl >= L.n_internal + L.n || cr >= L.n_internal + L.n ||
-                (cl != from && cr != from)) {
+            old = arrive_acq_rel(&bd[node].flag);
+            if (old == 0) break;                // first arrival: the sibling finishes
+        }
+        if (cl < 0 || cr < 0 || cl >= L.n_internal + L.n || cr >= L.n_internal + L.n ||
+            (cl != from && cr != from)) {
+            atomicOr(status, GCS_DEV_TREE_MALFORMED);
+            break;
+        }
+        const bool left = cl == from;
+        const int sib = left ? cr : cl;
+        // a local node's internal children are local too: read them from
+        // shared memory (their own range end is inside the block)
+        ChildData other;
+        if (local && sib < L.n_internal) {
+            const int so = sib + s - b0;
+            if (so < 0 || so >= kAggThreads) {
                 atomicOr(status, GCS_DEV_TREE_MALFORMED);
                 break;
             }
-            const bool left = cl == from;
-            const ChildData other = load_child(left ? cr : cl, L.n_internal, pos, tr, bd, com64, fp64);
-            const ChildData& A = left ? mine : other;   // left child
-            const ChildData& B = left ? other : mine;   // right child
-            const float3 lo = make_float3(fminf(A.lo.x, B.lo.x), fminf(A.lo.y, B.lo.y),
-                                          fminf(A.lo.z, B.lo.z));
-            const float3 hi = make_float3(fmaxf(A.hi.x, B.hi.x), fmaxf(A.hi.y, B.hi.y),
-                                          fmaxf(A.hi.z, B.hi.z));
-            const float width = fmaxf(__fsub_rn(hi.x, lo.x),
-                                      fmaxf(__fsub_rn(hi.y, lo.y), __fsub_rn(hi.z, lo.z)));
-            const float m = __fadd_rn(A.m, B.m);
-            float3 com;
-            if (m > 0.0f) {
-                if (fp64) {
-                    const double md = A.md + B.md;
-                    const double3 mx = make_double3(A.mx.x + B.mx.x, A.mx.y + B.mx.y, A.mx.z + B.mx.z);
-                    com = make_float3((float)(mx.x / md), (float)(mx.y / md), (float)(mx.z / md));
-                    com64[node] = make_double4(mx.x, mx.y, mx.z, md);
-                } else {
-                    com = make_float3(com_fp32(A.com.x, A.m, B.com.x, B.m, m),
-                                      com_fp32(A.com.y, A.m, B.com.y, B.m, m),
-                                      com_fp32(A.com.z, A.m, B.com.z, B.m, m));
-                }
-            } else {
-                com = make_float3(__fmul_rn(__fadd_rn(lo.x, hi.x), 0.5f),
-                                  __fmul_rn(__fadd_rn(lo.y, hi.y), 0.5f),
-                                  __fmul_rn(__fadd_rn(lo.z, hi.z), 0.5f));
-                if (fp64) com64[node] = make_double4(0.0, 0.0, 0.0, 0.0);
-            }
-            float4* t4 = reinterpret_cast<float4*>(tr + node);
-            t4[0] = make_float4(com.x, com.y, com.z, m);
-            tr[node].width = width;
-            float4* b4 = reinterpret_cast<float4*>(bd + node);
-            b4[0] = make_float4(lo.x, lo.y, lo.z, hi.x);
-            reinterpret_cast<float2*>(b4 + 1)[0] = make_float2(hi.y, hi.z);
-            ChildData next;
-            next.lo = lo;
-            next.hi = hi;
-            next.com = com;
-            next.m = m;
-            if (fp64) {
-                const bool pos_mass = m > 0.0f;
-                next.md = pos_mass ? A.md + B.md : 0.0;
-                next.mx = pos_mass ? make_double3(A.mx.x + B.mx.x, A.mx.y + B.mx.y, A.mx.z + B.mx.z)
-                                   : make_double3(0.0, 0.0, 0.0);
-            }
-            mine = next;
-            from = node;
-            node = up;
+            other = from_local(snode[so]);
+        } else {
+            other = load_child(sib, L.n_internal, pos, tr, bd, com64, fp64);
         }
+        const ChildData& A = left ? mine : other;   // left child
+        const ChildData& B = left ? other : mine;   // right child
+        const float3 lo = make_float3(fminf(A.lo.x, B.lo.x), fminf(A.lo.y, B.lo.y),
+                                      fminf(A.lo.z, B.lo.z));
+        const float3 hi = make_float3(fmaxf(A.hi.x, B.hi.x), fmaxf(A.hi.y, B.hi.y),
+                                      fmaxf(A.hi.z, B.hi.z));
+        const float width = fmaxf(__fsub_rn(hi.x, lo.x),
+                                  fmaxf(__fsub_rn(hi.y, lo.y), __fsub_rn(hi.z, lo.z)));
+        const float m = __fadd_rn(A.m, B.m);
+        float3 com;
+        ChildData next;
+        next.md = 0.0;
+        next.mx = make_double3(0.0, 0.0, 0.0);
+        if (m > 0.0f) {
+            if (fp64) {
+                next.md = A.md + B.md;
+                next.mx = make_double3(A.mx.x + B.mx.x, A.mx.y + B.mx.y, A.mx.z + B.mx.z);
+                com = make_float3((float)(next.mx.x / next.md), (float)(next.mx.y / next.md),
+                                  (float)(next.mx.z / next.md));
+            } else {
+                com = make_float3(com_fp32(A.com.x, A.m, B.com.x, B.m, m),
+                                  com_fp32(A.com.y, A.m, B.com.y, B.m, m),
+                                  com_fp32(A.com.z, A.m, B.com.z, B.m, m));
+            }
+        } else {
+            com = make_float3(__fmul_rn(__fadd_rn(lo.x, hi.x), 0.5f),
+                              __fmul_rn(__fadd_rn(lo.y, hi.y), 0.5f),
+                              __fmul_rn(__fadd_rn(lo.z, hi.z), 0.5f));
+        }
+        if (fp64) com64[node] = make_double4(next.mx.x, next.mx.y, next.mx.z, next.md);
+        float4* t4 = reinterpret_cast<float4*>(tr + node);
+        t4[0] = make_float4(com.x, com.y, com.z, m);
+        tr[node].width = width;
+        float4* b4 = reinterpret_cast<float4*>(bd + node);
+        b4[0] = make_float4(lo.x, lo.y, lo.z, hi.x);
+        reinterpret_cast<float2*>(b4 + 1)[0] = make_float2(hi.y, hi.z);
+        next.lo = lo;
+        next.hi = hi;
+        next.com = com;
+        next.m = m;
+        if (local) {
+            LocalNode& q = snode[own - b0];
+            q.lo = lo;
+            q.hi = hi;
+            q.com = com;
+            q.m = m;
+            q.mx = next.mx;
+            q.md = next.md;
+        }
+        mine = next;
+        from = node;
+        node = up;
     }
 }
 
@@ -255,7 +317,8 @@ void launch_aggregate(const Layout& L, const float4* pos, BvhNodeTraverse* tr, B
                       double4* com64, const int32_t* leaf_parent, int com_fp64, uint32_t* status,
                       cudaStream_t st) {
     if (L.n <= 0) return;
-    aggregate_kernel<<<tree_grid(L.n), 256, 0, st>>>(L, pos, tr, bd, com64, leaf_parent, com_fp64, status);
+    aggregate_kernel<<<tree_grid(L.n), kAggThreads, 0, st>>>(L, pos, tr, bd, com64, leaf_parent, com_fp64,
+                                                             status);
 }
 
 }  // namespace gcs
