@@ -40,6 +40,16 @@ struct gcs_ctx {
     int sorted_buf = 0;
     BvhNodeTraverse* tr = nullptr;
     BvhNodeBuild* bd = nullptr;
+    // Walk records (one per internal node) and what they were written for:
+    // the aggregation of generation wn_gen with G = wn_G and leaf size wn_L.
+    // tree_gen counts enqueued aggregations and layout changes, so a walk
+    // whose records are older than the tree, or were written for another G
+    // or leaf size, first rewrites them from the traverse records.
+    WalkNode* wn = nullptr;
+    uint64_t tree_gen = 1;
+    uint64_t wn_gen = 0;
+    float wn_G = 0.0f;
+    int32_t wn_L = 0;
     double4* com64 = nullptr;
     int32_t* leaf_parent = nullptr;
     int64_t* seg_off = nullptr;
@@ -163,7 +173,7 @@ void drop_graphs(gcs_ctx* c) {
 void free_all(gcs_ctx* c) {
     drop_graphs(c);
     void* ptrs[] = {c->pos[0], c->pos[1], c->vel[0], c->vel[1], c->acc, c->keys[0], c->keys[1],
-                    c->idx[0], c->idx[1], c->tr, c->bd, c->com64, c->leaf_parent, c->seg_off,
+                    c->idx[0], c->idx[1], c->tr, c->bd, c->wn, c->com64, c->leaf_parent, c->seg_off,
                     c->seg_id, c->groups, c->chunks, c->seg_bounds, c->staging, c->pb_staging,
                     c->scratch, c->status, c->diag, c->targets, c->direct_out, c->counts,
                     c->walk_stack};
@@ -192,6 +202,14 @@ int validate_params(gcs_ctx* c, const gcs_params* p) {
 }
 
 int default_walk_batch() { return 32; }
+
+WalkNodeParams walk_node_params(const gcs_ctx* c, const gcs_params* p) {
+    WalkNodeParams w;
+    w.wn = c->wn;
+    w.G = p->G;
+    w.leaf_size = std::min(std::max(p->leaf_size, 1), 32);
+    return w;
+}
 
 // Walk work units: runs of <= group_width consecutive particles that never
 // straddle a segment, so a segment's groups are the same alone or batched.
@@ -266,10 +284,16 @@ static int run_stage(gcs_ctx* c, const gcs_params* p, int stage) {
         case GCS_STAGE_BUILD:
             launch_build(L, c->keys[c->sorted_buf], c->tr, c->bd, c->leaf_parent, c->status, st);
             return check_launch(c, "build");
-        case GCS_STAGE_AGGREGATE:
-            launch_aggregate(L, c->pos[c->cur], c->tr, c->bd, c->com64, c->leaf_parent, p->com_fp64,
+        case GCS_STAGE_AGGREGATE: {
+            const WalkNodeParams wnp = walk_node_params(c, p);
+            launch_aggregate(L, c->pos[c->cur], c->tr, c->bd, c->com64, c->leaf_parent, p->com_fp64, wnp,
                              c->status, st);
+            c->tree_gen++;
+            c->wn_gen = c->tree_gen;
+            c->wn_G = wnp.G;
+            c->wn_L = wnp.leaf_size;
             return check_launch(c, "aggregate");
+        }
         case GCS_STAGE_WALK: {
             WalkParams wp;
             wp.G = p->G;
@@ -278,7 +302,14 @@ static int run_stage(gcs_ctx* c, const gcs_params* p, int stage) {
             wp.leaf_size = p->leaf_size;
             wp.batch = p->walk_batch > 0 ? p->walk_batch : default_walk_batch();
             wp.with_potential = p->with_potential ? 1 : 0;
-            launch_walk(L, wp, c->pos[c->cur], c->tr, c->groups, c->n_groups, c->acc,
+            const WalkNodeParams wnp = walk_node_params(c, p);
+            if (c->wn_gen != c->tree_gen || c->wn_G != wnp.G || c->wn_L != wnp.leaf_size) {
+                launch_walk_nodes(L, c->tr, wnp, c->status, st);
+                c->wn_gen = c->tree_gen;
+                c->wn_G = wnp.G;
+                c->wn_L = wnp.leaf_size;
+            }
+            launch_walk(L, wp, c->pos[c->cur], c->wn, c->groups, c->n_groups, c->acc,
                         scratch_at<uint32_t>(c, sl.walk_q), c->status, p->walk_blocks_per_sm, c->sm_count,
                         c->count_walk ? c->counts : nullptr, c->walk_stack, c->walk_stack_entries, st);
             return check_launch(c, "walk");
@@ -389,6 +420,7 @@ int gcs_create(gcs_ctx** out, int64_t capacity, int32_t max_segments, int32_t de
     }
     cudaMemset(c->scratch, 0, c->scratch_cap);  // the walk queue starts (and stays) at zero
     cudaMemset(c->status, 0, sizeof(uint32_t));
+    cudaMemset(c->wn, 0, sizeof(WalkNode) * (size_t)capacity);  // codes of unwritten records stay in range
     cudaMemset(c->acc, 0, sizeof(float4) * (size_t)capacity);
     int64_t cnt = capacity;
     rc = gcs_set_segments(c, 1, &cnt);
@@ -442,6 +474,7 @@ static int allocate_state(gcs_ctx* c) {
     if (!rc) rc |= dalloc(c, &c->acc, N);
     if (!rc) rc |= dalloc(c, &c->tr, N);
     if (!rc) rc |= dalloc(c, &c->bd, N);
+    if (!rc) rc |= dalloc(c, &c->wn, N);
     if (!rc) rc |= dalloc(c, &c->com64, N);
     if (!rc) rc |= dalloc(c, &c->leaf_parent, N);
     if (!rc) rc |= dalloc(c, &c->seg_off, (size_t)max_segments + 1);
@@ -535,6 +568,7 @@ static int apply_layout(gcs_ctx* c, int32_t num_segments, const int64_t* counts)
     c->nseg = num_segments;
     c->n_internal = (int32_t)(n - num_segments);
     c->n_chunks = (int)chunks.size();
+    c->tree_gen++;  // the tree (and its walk records) belong to the old layout
     drop_graphs(c);
     return upload_groups(c);
 }

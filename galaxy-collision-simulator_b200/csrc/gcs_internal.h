@@ -6,7 +6,8 @@
 //                                         the byte order of Star bytes 28..31)
 //   acc      float4 ax,ay,az,potential
 //   keys[2]  u64 Morton codes, idx[2] u32 positions (radix-sort ping-pong)
-//   nodes_tr BvhNodeTraverse[n_internal], nodes_bd BvhNodeBuild[n_internal]
+//   nodes_tr BvhNodeTraverse[n_internal], nodes_bd BvhNodeBuild[n_internal],
+//   wn       WalkNode[n_internal] (walk records: com, G*mass, width^2, codes)
 //   com64    double4 [n_internal] FP64 mass-weighted position sums
 //   leaf_parent i32[N]
 //   seg_off  i64[S+1], seg_id i32[N], groups int4[n_groups]
@@ -90,9 +91,10 @@ void launch_gather(const uint32_t* idx, const float4* pos_in, const float4* vel_
                    float4* vel_out, int64_t n, cudaStream_t st);
 void launch_build(const Layout& L, const uint64_t* keys, BvhNodeTraverse* tr, BvhNodeBuild* bd,
                   int32_t* leaf_parent, uint32_t* status, cudaStream_t st);
+struct WalkNodeParams;
 void launch_aggregate(const Layout& L, const float4* pos, BvhNodeTraverse* tr, BvhNodeBuild* bd,
-                      double4* com64, const int32_t* leaf_parent, int com_fp64, uint32_t* status,
-                      cudaStream_t st);
+                      double4* com64, const int32_t* leaf_parent, int com_fp64, const WalkNodeParams& wnp,
+                      uint32_t* status, cudaStream_t st);
 
 struct WalkParams {
     float G, eps2, theta2;
@@ -100,13 +102,42 @@ struct WalkParams {
     int32_t batch;
     int32_t with_potential;
 };
+
+// Walk record of one internal node (32 bytes, two 16-byte loads), written
+// beside the node's BvhNodeTraverse record for a given G and leaf size L:
+//   cm    com.x, com.y, com.z, G*mass
+//   link  bits(width^2), code_a, code_b, 0 where
+//           code_b >= kWalkBucketTag  the node holds <= L particles, summed
+//                                     directly: [code_a, code_a + code_b - tag)
+//           code_b == kWalkSkipTag    malformed links: nothing below it
+//           otherwise                 children: >= 0 internal node,
+//                                     < 0 particle ~code
+// Every code names an index below the context's capacity, so a walk over
+// stale records reads inside its arrays.
+struct WalkNode {
+    float4 cm;
+    int4 link;
+};
+static_assert(sizeof(WalkNode) == 32, "WalkNode must be 32 bytes");
+constexpr int kWalkBucketTag = 1 << 30;
+constexpr int kWalkSkipTag = 0x7FFFFFFF;
+// G and leaf size of the walk records an aggregation writes (wn null: none).
+struct WalkNodeParams {
+    WalkNode* wn;
+    float G;
+    int32_t leaf_size;  // 1..32
+};
+// Walk records of every internal node from the traverse records (when the
+// walk runs with a G or leaf size other than the aggregation's).
+void launch_walk_nodes(const Layout& L, const BvhNodeTraverse* tr, WalkNodeParams wnp, uint32_t* status,
+                       cudaStream_t st);
 // Global-memory stack entries (int2) per walk warp: the shared-memory stack
 // spills its bottom here.  A round adds at most `batch` entries per tree
 // level, so 8192 covers batch 64 on trees 128 levels deep.
 constexpr int kWalkGlobalStack = 8192;
 constexpr int kWalkMaxBatch = 64;  // nodes popped per walk round
 void launch_walk(const Layout& L, const WalkParams& wp, const float4* pos,
-                 const BvhNodeTraverse* tr, const WalkGroup* groups, int n_groups,
+                 const WalkNode* wn, const WalkGroup* groups, int n_groups,
                  float4* acc, uint32_t* queue, uint32_t* status, int blocks_per_sm,
                  int sm_count, unsigned long long* counts, int2* gstack, size_t gstack_entries,
                  cudaStream_t st);

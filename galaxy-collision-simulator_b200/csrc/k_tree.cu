@@ -164,6 +164,54 @@ __device__ __forceinline__ ChildData from_local(const LocalNode& q) {
     return r;
 }
 
+// Walk record of internal node `node` (links already range-checked): the
+// particle range [min(own, re), max(own, re)] clipped to the segment
+// [seg_lo, seg_hi]; <= leaf_size particles make a bucket, else the children
+// are coded as internal node or ~particle.
+__device__ __forceinline__ void write_walk_node(const WalkNodeParams& wnp, int node, float3 com, float m,
+                                                float width, int cl, int cr, int own, int re, int seg_lo,
+                                                int seg_hi, int n_internal) {
+    const int lo = max(min(own, re), seg_lo);
+    const int cnt = min(max(own, re), seg_hi) - lo + 1;
+    int ca, cb;
+    if (cnt <= wnp.leaf_size) {
+        ca = lo;
+        cb = kWalkBucketTag + max(cnt, 0);
+    } else {
+        ca = cl >= n_internal ? ~(cl - n_internal) : cl;
+        cb = cr >= n_internal ? ~(cr - n_internal) : cr;
+    }
+    float4* w = reinterpret_cast<float4*>(wnp.wn + node);
+    w[0] = make_float4(com.x, com.y, com.z, __fmul_rn(wnp.G, m));
+    reinterpret_cast<int4*>(w)[1] = make_int4(__float_as_int(__fmul_rn(width, width)), ca, cb, 0);
+}
+
+// Walk records from the traverse records: one thread per particle g; the
+// internal node g - s exists for every particle but the last of segment s.
+__global__ void walk_nodes_kernel(Layout L, const BvhNodeTraverse* __restrict__ tr, WalkNodeParams wnp,
+                                  uint32_t* __restrict__ status) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= L.n) return;
+    const int s = L.nseg > 1 ? __ldg(L.seg_id + g) : 0;
+    const int seg_lo = (int)__ldg(L.seg_off + s), seg_hi = (int)__ldg(L.seg_off + s + 1) - 1;
+    if (g >= seg_hi) return;
+    const int node = g - s;
+    const float4* np = reinterpret_cast<const float4*>(tr + node);
+    const float4 a = __ldg(np);
+    const float4 c = __ldg(np + 1);
+    const int cl = __float_as_int(c.y), cr = __float_as_int(c.z);
+    const int lim = L.n_internal + L.n;
+    if (cl >= 0 && cl < lim && cr >= 0 && cr < lim) {
+        write_walk_node(wnp, node, make_float3(a.x, a.y, a.z), a.w, c.x, cl, cr, node + s, __float_as_int(c.w),
+                        seg_lo, seg_hi, L.n_internal);
+    } else {
+        atomicOr(status, GCS_DEV_BUILD_RANGE);
+        float4* w = reinterpret_cast<float4*>(wnp.wn + node);
+        w[0] = make_float4(a.x, a.y, a.z, __fmul_rn(wnp.G, a.w));
+        reinterpret_cast<int4*>(w)[1] = make_int4(__float_as_int(__fmul_rn(c.x, c.x)), 0, kWalkSkipTag, 0);
+    }
+}
+
 // One thread per particle; block b owns particles [256 b, 256 b + 256).  A
 // node whose particle range lies inside its block's range has both children
 // finished by threads of that block: its arrival counter and the finished
@@ -174,7 +222,7 @@ __global__ void __launch_bounds__(kAggThreads, 4)
 aggregate_kernel(Layout L, const float4* __restrict__ pos,
                                  BvhNodeTraverse* __restrict__ tr, BvhNodeBuild* __restrict__ bd,
                                  double4* __restrict__ com64, const int32_t* __restrict__ leaf_parent,
-                                 int com_fp64, uint32_t* __restrict__ status) {
+                                 int com_fp64, WalkNodeParams wnp, uint32_t* __restrict__ status) {
     __shared__ int sflag[kAggThreads];
     __shared__ LocalNode snode[kAggThreads];
     const bool fp64 = com_fp64 != 0;
@@ -184,6 +232,7 @@ aggregate_kernel(Layout L, const float4* __restrict__ pos,
     const int g = b0 + threadIdx.x;
     if (g >= L.n) return;
     const int s = L.nseg > 1 ? __ldg(L.seg_id + g) : 0;
+    const int seg_lo = (int)__ldg(L.seg_off + s), seg_hi = (int)__ldg(L.seg_off + s + 1) - 1;
     // The node this thread has just finished (first the leaf itself) is
     // carried in registers; at each parent only the sibling is loaded.
     int from = L.n_internal + g;
@@ -278,6 +327,7 @@ aggregate_kernel(Layout L, const float4* __restrict__ pos,
         float4* t4 = reinterpret_cast<float4*>(tr + node);
         t4[0] = make_float4(com.x, com.y, com.z, m);
         tr[node].width = width;
+        if (wnp.wn) write_walk_node(wnp, node, com, m, width, cl, cr, own, re, seg_lo, seg_hi, L.n_internal);
         float4* b4 = reinterpret_cast<float4*>(bd + node);
         b4[0] = make_float4(lo.x, lo.y, lo.z, hi.x);
         reinterpret_cast<float2*>(b4 + 1)[0] = make_float2(hi.y, hi.z);
@@ -314,11 +364,17 @@ void launch_build(const Layout& L, const uint64_t* keys, BvhNodeTraverse* tr, Bv
 }
 
 void launch_aggregate(const Layout& L, const float4* pos, BvhNodeTraverse* tr, BvhNodeBuild* bd,
-                      double4* com64, const int32_t* leaf_parent, int com_fp64, uint32_t* status,
-                      cudaStream_t st) {
+                      double4* com64, const int32_t* leaf_parent, int com_fp64, const WalkNodeParams& wnp,
+                      uint32_t* status, cudaStream_t st) {
     if (L.n <= 0) return;
     aggregate_kernel<<<tree_grid(L.n), kAggThreads, 0, st>>>(L, pos, tr, bd, com64, leaf_parent, com_fp64,
-                                                             status);
+                                                             wnp, status);
+}
+
+void launch_walk_nodes(const Layout& L, const BvhNodeTraverse* tr, WalkNodeParams wnp, uint32_t* status,
+                       cudaStream_t st) {
+    if (L.n <= 0 || !wnp.wn) return;
+    walk_nodes_kernel<<<tree_grid(L.n), 256, 0, st>>>(L, tr, wnp, status);
 }
 
 }  // namespace gcs

@@ -18,19 +18,21 @@
 // warp walks the tree once for its group with one stack; each stack entry
 // carries the mask of lanes that still need that subtree, and each lane
 // takes its own opening decision, so the group walk is the union of the 32
-// per-target walks with no change to any target's terms.  Each round:
-//   1. up to `batch` (<= 32*H) entries are popped; lane k fetches nodes k and
-//      k+32 (two 16-byte loads each) and digests them: G*mass, width^2, and
-//      either the particle range to sum (a node of <= L particles) or its two
-//      children coded as node or particle;
+// per-target walks with no change to any target's terms.  Nodes are read
+// from walk records (WalkNode: centre of mass and G*mass, width^2, and the
+// children or the bucket range for the step's leaf size), which the
+// aggregation writes beside the traverse records.  Each round:
+//   1. up to `batch` (<= 32*H) entries are popped; lane k fetches the
+//      records of nodes k and k+32 (two 16-byte loads each);
 //   2. each node is classified against the group's bounding box with a
 //      2^-16 relative margin: "take" if every lane of the box must accept
 //      it, "open" if every lane must open it, else "mixed" (the margin is far
 //      above the few-ulp rounding of any lane's own d2, so a class never
 //      contradicts a lane's own test);
-//   3. take nodes go through a monopole-only loop, mixed nodes through the
-//      per-lane opening test (a predicated monopole and a ballot of opening
-//      lanes), open nodes skip evaluation altogether;
+//   3. take nodes whose mask holds every live lane go through a monopole
+//      loop without lane masks, other take nodes through a masked one, mixed
+//      nodes through the per-lane opening test (a predicated monopole and a
+//      ballot of opening lanes); open nodes skip evaluation altogether;
 //   4. in parallel, each lane pushes its nodes' internal children and
 //      appends their particle sources (leaf children, or the whole range of
 //      a small node) at offsets from one warp prefix scan;
@@ -59,19 +61,15 @@ constexpr int kWalkThreads = kWalkWarps * 32;
 constexpr int kSpillCount = 128;  // entries moved per spill / refill
 constexpr int kSrcCap = 64;
 constexpr uint32_t kFull = 0xFFFFFFFFu;
-// Digested node codes (code_a / code_b):
-//   code_b >= kBucketTag   the node itself is summed directly: particles
-//                          [code_a, code_a + code_b - kBucketTag)
-//   code_b == kSkipTag     no node, or malformed children: nothing pushed
-//   otherwise              children: >= 0 internal node, < 0 particle ~code
-constexpr int kBucketTag = 1 << 30;
-constexpr int kSkipTag = 0x7FFFFFFF;
+// Node codes come from the walk records (WalkNode: code_a / code_b with
+// kWalkBucketTag and kWalkSkipTag).
 
 // Classes of a batch node against the group's bounding box.
-constexpr int kClassNone = 0;   // lane holds no node
-constexpr int kClassTake = 1;   // every lane of the group accepts it
-constexpr int kClassOpen = 2;   // every lane of the group opens it
-constexpr int kClassMixed = 3;  // lanes decide one by one
+constexpr int kClassNone = 0;      // lane holds no node
+constexpr int kClassTake = 1;      // every lane of the group accepts it
+constexpr int kClassOpen = 2;      // every lane of the group opens it
+constexpr int kClassMixed = 3;     // lanes decide one by one
+constexpr int kClassTakeFull = 4;  // kClassTake, and every live lane is in its mask
 constexpr float kBoxLo = 1.0f - 1.0f / 65536.0f;
 constexpr float kBoxHi = 1.0f + 1.0f / 65536.0f;
 
@@ -84,7 +82,7 @@ constexpr float kBoxHi = 1.0f + 1.0f / 65536.0f;
 template <int H>
 struct WarpSmem {
     static constexpr int kBatch = 32 * H;
-    static constexpr int kPairs = kBatch / 2 + 1;                  // two padded lists
+    static constexpr int kPairs = kBatch / 2 + 2;                  // three padded lists
     static constexpr int kStackCap = 256 + 64 * H;                 // stack entries
     static constexpr int kSpillAbove = kStackCap - 2 * kBatch;     // a round pushes <= 2*batch
     int2 stk[kStackCap];          // node, lane mask
@@ -144,6 +142,18 @@ __device__ __forceinline__ PairD pair_d(float4 xy, float4 zm, float2 npx, float2
     r.dy = __fadd2_rn(make_float2(xy.z, xy.w), npy);
     r.dz = __fadd2_rn(make_float2(zm.x, zm.y), npz);
     r.d2 = softened_d2_x2(r.dx, r.dy, r.dz, e2);
+    return r;
+}
+
+// pair_d for nodes every lane of the entry accepts: no opening decision
+// depends on d2 here, so eps^2 starts the FMA chain (d2 differs from the
+// decision form by rounding only).
+__device__ __forceinline__ PairD pair_d_take(float4 xy, float4 zm, float2 npx, float2 npy, float2 npz, float2 e2) {
+    PairD r;
+    r.dx = __fadd2_rn(make_float2(xy.x, xy.y), npx);
+    r.dy = __fadd2_rn(make_float2(xy.z, xy.w), npy);
+    r.dz = __fadd2_rn(make_float2(zm.x, zm.y), npz);
+    r.d2 = __ffma2_rn(r.dz, r.dz, __ffma2_rn(r.dy, r.dy, __ffma2_rn(r.dx, r.dx, e2)));
     return r;
 }
 
@@ -243,7 +253,7 @@ __device__ __forceinline__ uint32_t warp_exclusive_scan(uint32_t v, int lane) {
 template <int H, bool kPot, bool kCount>
 __global__ void __launch_bounds__(kWalkThreads, WalkOcc<H>::kMinBlocks)
 walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
-            const BvhNodeTraverse* __restrict__ tr, const WalkGroup* __restrict__ groups,
+            const WalkNode* __restrict__ wn, const WalkGroup* __restrict__ groups,
             int n_groups, float4* __restrict__ acc, uint32_t* __restrict__ queue,
             uint32_t* __restrict__ status, unsigned long long* __restrict__ counts,
             int2* __restrict__ gstack, int gstack_cap) {
@@ -258,10 +268,10 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
     const float G = wp.G, eps2 = wp.eps2, theta2 = wp.theta2;
     const float2 e2 = make_float2(eps2, eps2), th2 = make_float2(theta2, theta2);
     const float leaf_thr = __fmul_rn(eps2, 1.01f);
-    const int leaf_size = wp.leaf_size;
     const int batch = wp.batch;
-    const int n_internal = L.n_internal;
-    const int n_total = L.n;
+    // box classification thresholds: take iff w^2 < s2min * k_take, open iff
+    // w^2 >= s2max * k_open (theta^2 with the 2^-16 relative margin)
+    const float k_take = theta2 * kBoxLo, k_open = theta2 * kBoxHi;
 
     for (;;) {
         int g = 0;
@@ -288,7 +298,6 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
         const int s = grp.seg;
         const int off = (int)__ldg(L.seg_off + s);
         const int seg_n = (int)__ldg(L.seg_off + s + 1) - off;
-        const int seg_end = off + seg_n;
         Accum A;
         A.ax = A.ay = A.az = A.pot = make_float2(0.f, 0.f);
         A.n_mono = A.n_part = A.w_node = A.w_src = A.rounds = A.spills = A.all_open = A.all_take = 0u;
@@ -326,7 +335,7 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                     break;
                 }
                 top -= b;
-                // 1-2. fetch, digest and classify nodes lane and lane+32
+                // 1-2. fetch and classify nodes lane and lane+32
                 int code_a[H], code_b[H], cls[H];
                 uint32_t my_mask[H];
                 float4 com[H];
@@ -335,37 +344,24 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                 for (int h = 0; h < H; ++h) {
                     const int j = lane + 32 * h;
                     code_a[h] = 0;
-                    code_b[h] = kSkipTag;
+                    code_b[h] = kWalkSkipTag;
                     cls[h] = kClassNone;
                     my_mask[h] = 0u;
                     com[h] = make_float4(0.f, 0.f, 0.f, 0.f);
                     w2[h] = 0.0f;
                     if (j < b) {
                         const int2 e = W.stk[top + j];
-                        const float4* np = reinterpret_cast<const float4*>(tr + e.x);
-                        float4 a = __ldg(np);
-                        const float4 c = __ldg(np + 1);
-                        a.w = __fmul_rn(G, a.w);
-                        const int own = e.x + s;  // particle index at this end of the range
-                        const int re = __float_as_int(c.w);
-                        const int lo = max(min(own, re), off);
-                        const int cnt = min(max(own, re), seg_end - 1) - lo + 1;
-                        if (cnt <= leaf_size) {
-                            code_a[h] = lo;
-                            code_b[h] = kBucketTag + max(cnt, 0);
-                        } else {
-                            const int cl = __float_as_int(c.y), cr = __float_as_int(c.z);
-                            if (cl >= 0 && cl < n_internal + n_total && cr >= 0 && cr < n_internal + n_total) {
-                                code_a[h] = cl >= n_internal ? ~(cl - n_internal) : cl;
-                                code_b[h] = cr >= n_internal ? ~(cr - n_internal) : cr;
-                            } else {
-                                atomicOr(status, GCS_DEV_BUILD_RANGE);
-                            }
-                        }
-                        w2[h] = __fmul_rn(c.x, c.x);
+                        const float4* np = reinterpret_cast<const float4*>(wn + e.x);
+                        const float4 a = __ldg(np);
+                        const int4 k = __ldg(reinterpret_cast<const int4*>(np + 1));
+                        w2[h] = __int_as_float(k.x);
+                        code_a[h] = k.y;
+                        code_b[h] = k.z;
                         com[h] = a;
                         my_mask[h] = (uint32_t)e.y;
-                        float s2min = 0.0f, s2max = 0.0f;
+                        // squared softened distances from the centre of mass
+                        // to the nearest and farthest points of the box
+                        float s2min = eps2, s2max = eps2;
                         {
                             const float dl[3] = {box_lo.x - a.x, box_lo.y - a.y, box_lo.z - a.z};
                             const float dh[3] = {a.x - box_hi.x, a.y - box_hi.y, a.z - box_hi.z};
@@ -377,31 +373,37 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                                 s2max = fmaf(far, far, s2max);
                             }
                         }
-                        if (w2[h] < theta2 * (s2min + eps2) * kBoxLo) cls[h] = kClassTake;
-                        else if (w2[h] >= theta2 * (s2max + eps2) * kBoxHi) cls[h] = kClassOpen;
+                        if (w2[h] < s2min * k_take) cls[h] = my_mask[h] == live ? kClassTakeFull : kClassTake;
+                        else if (w2[h] >= s2max * k_open) cls[h] = kClassOpen;
                         else cls[h] = kClassMixed;
                     }
                 }
-                // compact: take nodes first, then mixed ones
-                uint32_t bt[H], bm[H];
-                int n_take = 0, n_mixed = 0;
+                // compact into three pair-interleaved lists, each starting at
+                // an even slot: take nodes with every live lane in their mask,
+                // other take nodes, mixed nodes; odd lists end with an empty
+                // entry
+                uint32_t bf[H], bt[H], bm[H];
+                int n_full = 0, n_take = 0, n_mixed = 0;
 #pragma unroll
                 for (int h = 0; h < H; ++h) {
+                    bf[h] = __ballot_sync(kFull, cls[h] == kClassTakeFull);
                     bt[h] = __ballot_sync(kFull, cls[h] == kClassTake);
                     bm[h] = __ballot_sync(kFull, cls[h] == kClassMixed);
+                    n_full += __popc(bf[h]);
                     n_take += __popc(bt[h]);
                     n_mixed += __popc(bm[h]);
                 }
-                // take nodes in slots [0, n_take), mixed nodes from the next
-                // even slot; odd lists are padded with an empty entry
-                const int mixed_base = (n_take + 1) & ~1;
+                const int take_base = (n_full + 1) & ~1;
+                const int mixed_base = (take_base + n_take + 1) & ~1;
                 int slot[H];
                 {
-                    int take_before = 0, mixed_before = 0;
+                    int full_before = 0, take_before = 0, mixed_before = 0;
 #pragma unroll
                     for (int h = 0; h < H; ++h) {
-                        slot[h] = cls[h] == kClassTake ? take_before + __popc(bt[h] & lt)
-                                : (cls[h] == kClassMixed ? mixed_base + mixed_before + __popc(bm[h] & lt) : -1);
+                        slot[h] = cls[h] == kClassTakeFull ? full_before + __popc(bf[h] & lt)
+                                : cls[h] == kClassTake ? take_base + take_before + __popc(bt[h] & lt)
+                                : cls[h] == kClassMixed ? mixed_base + mixed_before + __popc(bm[h] & lt) : -1;
+                        full_before += __popc(bf[h]);
                         take_before += __popc(bt[h]);
                         mixed_before += __popc(bm[h]);
                         if (slot[h] >= 0) {
@@ -410,8 +412,9 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                         }
                     }
                     const float4 empty = make_float4(1e30f, 1e30f, 1e30f, 0.0f);
-                    const int pad = lane == 0 ? ((n_take & 1) ? n_take : -1)
-                                  : lane == 1 ? ((n_mixed & 1) ? mixed_base + n_mixed : -1) : -1;
+                    const int pad = lane == 0 ? ((n_full & 1) ? n_full : -1)
+                                  : lane == 1 ? ((n_take & 1) ? take_base + n_take : -1)
+                                  : lane == 2 ? ((n_mixed & 1) ? mixed_base + n_mixed : -1) : -1;
                     if (pad >= 0) {
                         put_pair(W.pxy, W.pzm, W.pmask, pad, empty, 0u);
                         reinterpret_cast<float*>(W.pw2 + (pad >> 1))[1] = 0.0f;
@@ -421,21 +424,29 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                 if (kCount) {
                     A.w_node += (uint32_t)b;
                     A.rounds += 1u;
-                    A.all_open += (uint32_t)(b - n_take - n_mixed);
-                    A.all_take += (uint32_t)n_take;
+                    A.all_open += (uint32_t)(b - n_full - n_take - n_mixed);
+                    A.all_take += (uint32_t)(n_full + n_take);
                 }
-                // 3a. nodes every lane accepts: monopole terms only, two
-                // nodes per packed evaluation
+                // 3a. nodes every live lane accepts: monopole terms, two
+                // nodes per packed evaluation, no lane masks
 #pragma unroll 2
-                for (int q = 0; q < ((n_take + 1) >> 1); ++q) {
+                for (int q = 0; q < (take_base >> 1); ++q) {
+                    const float4 zm = W.pzm[q];
+                    const PairD d = pair_d_take(W.pxy[q], zm, npx, npy, npz, e2);
+                    pair_add<kPot>(A, d, zm, true, true);
+                }
+                if (kCount && valid) A.n_mono += (uint32_t)n_full;
+                // 3b. nodes accepted by every lane of their mask
+#pragma unroll 2
+                for (int q = take_base >> 1; q < (mixed_base >> 1); ++q) {
                     const float4 zm = W.pzm[q];
                     const uint2 mk = W.pmask[q];
-                    const PairD d = pair_d(W.pxy[q], zm, npx, npy, npz, e2);
+                    const PairD d = pair_d_take(W.pxy[q], zm, npx, npy, npz, e2);
                     const bool use0 = (mk.x & lane_bit) != 0u, use1 = (mk.y & lane_bit) != 0u;
                     pair_add<kPot>(A, d, zm, use0, use1);
                     if (kCount) A.n_mono += (use0 ? 1u : 0u) + (use1 ? 1u : 0u);
                 }
-                // 3b. mixed nodes: each lane's own test; lane 0 records the
+                // 3c. mixed nodes: each lane's own test; lane 0 records the
                 // ballots of opening lanes for the nodes' owners
                 for (int q = mixed_base >> 1; q < ((mixed_base + n_mixed + 1) >> 1); ++q) {
                     const float4 zm = W.pzm[q];
@@ -462,9 +473,9 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                                : (cls[h] == kClassMixed ? reinterpret_cast<const uint32_t*>(W.pnopen)[slot[h]] : 0u);
                     n_push[h] = 0;
                     n_src[h] = 0;
-                    if (my_open[h] != 0u && code_b[h] != kSkipTag) {
-                        if (code_b[h] >= kBucketTag) {
-                            n_src[h] = code_b[h] - kBucketTag;
+                    if (my_open[h] != 0u && code_b[h] != kWalkSkipTag) {
+                        if (code_b[h] >= kWalkBucketTag) {
+                            n_src[h] = code_b[h] - kWalkBucketTag;
                         } else {
                             n_push[h] = (code_a[h] >= 0) + (code_b[h] >= 0);
                             n_src[h] = (code_a[h] < 0) + (code_b[h] < 0);
@@ -505,7 +516,7 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                         for (int j = j0; j < j1; ++j) {
                             const int r = j - first;  // r-th source of node h
                             int particle;
-                            if (code_b[h] >= kBucketTag) particle = code_a[h] + r;
+                            if (code_b[h] >= kWalkBucketTag) particle = code_a[h] + r;
                             else particle = (r == 0 && code_a[h] < 0) ? ~code_a[h] : ~code_b[h];
                             W.srcm[nsrc + (j - base)] = make_int2(particle, (int)my_open[h]);
                         }
@@ -636,7 +647,7 @@ size_t walk_stack_entries(int64_t grid_blocks) {
 }
 
 template <int H>
-static void launch_h(const Layout& L, const WalkParams& q, const float4* pos, const BvhNodeTraverse* tr,
+static void launch_h(const Layout& L, const WalkParams& q, const float4* pos, const WalkNode* tr,
                      const WalkGroup* groups, int n_groups, float4* acc, uint32_t* queue, uint32_t* status,
                      unsigned long long* counts, int2* gstack, unsigned g, cudaStream_t st) {
     const int cap = kWalkGlobalStack;
@@ -663,7 +674,7 @@ static void launch_h(const Layout& L, const WalkParams& q, const float4* pos, co
 }
 
 void launch_walk(const Layout& L, const WalkParams& wp, const float4* pos,
-                 const BvhNodeTraverse* tr, const WalkGroup* groups, int n_groups, float4* acc,
+                 const WalkNode* tr, const WalkGroup* groups, int n_groups, float4* acc,
                  uint32_t* queue, uint32_t* status, int blocks_per_sm, int sm_count,
                  unsigned long long* counts, int2* gstack, size_t gstack_entries, cudaStream_t st) {
     if (n_groups <= 0) return;
