@@ -87,18 +87,70 @@ def counts_for(n):
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle samples (200 ms) while the timed region runs."""
+    """SM clock and clock-event-reason samples taken while the timed region runs.
+
+    NVML is polled every 2 ms from a thread (the timed loops are ctypes calls,
+    which release the GIL); start() returns once the first sample is in, so
+    the samples cover the whole timed region.  Falls back to nvidia-smi's
+    200 ms loop when NVML cannot be loaded.
+    """
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    PERIOD_S = 0.002
 
     def __init__(self, device: int):
         self.device = device
         self.proc = None
         self.lines = []
+        self.nvml = None
+        self.handle = None
+        self.samples = []   # (sm_mhz, reasons bitmask)
+        self.sm_max = None
+        self.running = False
+
+    def _nvml_handle(self, nv):
+        import torch  # noqa: PLC0415
+        props = torch.cuda.get_device_properties(self.device)
+        uuid = getattr(props, "uuid", None)
+        if uuid is not None:
+            try:
+                u = str(uuid)
+                return nv.nvmlDeviceGetHandleByUUID(u if u.startswith("GPU-") else "GPU-" + u)
+            except Exception:  # noqa: BLE001
+                pass
+        return nv.nvmlDeviceGetHandleByIndex(self.device)
 
     def start(self):
+        try:
+            import pynvml as nv  # noqa: PLC0415
+            nv.nvmlInit()
+            self.handle = self._nvml_handle(nv)
+            self.sm_max = float(nv.nvmlDeviceGetMaxClockInfo(self.handle, nv.NVML_CLOCK_SM))
+            self.nvml = nv
+        except Exception:  # noqa: BLE001
+            self.nvml = None
+        if self.nvml is not None:
+            self.running = True
+            first = threading.Event()
+
+            def poll():
+                nv = self.nvml
+                while self.running:
+                    try:
+                        mhz = float(nv.nvmlDeviceGetClockInfo(self.handle, nv.NVML_CLOCK_SM))
+                        rs = int(nv.nvmlDeviceGetCurrentClocksEventReasons(self.handle))
+                        self.samples.append((mhz, rs))
+                    except Exception:  # noqa: BLE001
+                        pass
+                    first.set()
+                    time.sleep(self.PERIOD_S)
+
+            self.t = threading.Thread(target=poll, daemon=True)
+            self.t.start()
+            first.wait(timeout=2.0)
+            return
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
@@ -113,6 +165,22 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def stop(self):
+        if self.nvml is not None:
+            self.running = False
+            self.t.join(timeout=2)
+            nv = self.nvml
+            bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                    "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                    "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+            reasons = sorted({name for _, rs in self.samples for name, b in bits.items() if rs & b})
+            sm = [m for m, _ in self.samples]
+            try:
+                nv.nvmlShutdown()
+            except Exception:  # noqa: BLE001
+                pass
+            return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.sm_max,
+                    "reasons": reasons, "samples": len(sm), "source": "nvml, 2 ms"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -136,7 +204,7 @@ class ClockSampler:
                 if v.lower() == "active":
                     reasons.add(name)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi, 200 ms"}
 
 
 def measured_peaks():
