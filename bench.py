@@ -64,6 +64,7 @@ def parse():
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-render", action="store_true")
     ap.add_argument("--batched-count", type=int, default=256)
     ap.add_argument("--batched-steps", type=int, default=10)
     ap.add_argument("--no-served", action="store_true")
@@ -335,6 +336,52 @@ def _tune(gcs, ctx, leaf_max=32):
     q.tune_leaf_min = 4
     p, _ = ctx.autotune(q)
     return p
+
+
+def render_bench(gcs, torch, ctx, stream, frames=10, width=1920, height=1080):
+    """Headless splat frames of the context's current particles on the device:
+    accumulator clear + splat + resolve per frame, CUDA events on the stream,
+    for the reference's start-up camera and a close one; the oracle's
+    single-threaded CPU restatement timed on one frame for comparison."""
+    import ctypes as C  # noqa: PLC0415
+    n = ctx.n
+    out = torch.empty(width * height * 4, dtype=torch.uint8, device="cuda")
+    res = {"workload": "%d particles (the benchmark state), %dx%d RGBA8, fixed-point additive splat" % (n, width, height)}
+    cams = {"reference_camera": gcs.camera_reference()}
+    close = gcs.camera_reference()
+    close.pos[:] = (0.0, 30.0, 80.0)
+    close.front[:] = (0.0, -0.35, -1.0)
+    cams["close_camera"] = close
+    algo_bytes = 32.0 * n + (24 + 24 + 4) * width * height  # particles; clear, resolve read, RGBA write
+    for name, cam in cams.items():
+        def frame():
+            ctx.check(ctx.L.gcs_render_frame(ctx.handle, C.byref(cam), -1, width, height,
+                                             C.c_void_p(out.data_ptr()), 0))
+        for _ in range(3):
+            frame()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(frames):
+            frame()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / frames
+        res[name] = {"ms_per_frame": ms, "frames_per_s": 1e3 / ms,
+                     "algorithmic_gbs": algo_bytes / (ms / 1e3) / 1e9}
+    try:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle  # noqa: PLC0415
+        stars = ctx.download()
+        v, pm = gcs.camera_matrices(cams["reference_camera"], width, height)
+        t0 = time.perf_counter()
+        oracle.render(stars, v, pm, width, height)
+        res["cpu_oracle"] = {"ms_per_frame": 1e3 * (time.perf_counter() - t0), "cores": 1,
+                             "kind": "port", "sample": "one frame, reference start-up camera"}
+    except Exception as e:  # noqa: BLE001
+        res["cpu_oracle"] = {"unavailable": str(e)}
+    return res
 
 
 def batched_bench(gcs, torch, args):
@@ -650,6 +697,8 @@ def main():
             line["ref_gpu"] = ref_gpu_rate(stars)
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_reference_rate(stars, args.cpu_seconds)
+        if not args.no_render:
+            line["render"] = render_bench(gcs, torch, ctx, stream)
     ctx.close()
     if rank == 0 and world == 1:
         if not args.no_batched:

@@ -7,6 +7,7 @@
 // device), all work is asynchronous on the context's stream with no device
 // synchronisation between stages, and every failure is a status code.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -68,6 +69,11 @@ struct gcs_ctx {
     double* direct_out = nullptr;
     unsigned long long* counts = nullptr;  // walk interaction counters (count mode)
     int2* walk_stack = nullptr;            // per-warp global bottoms of the walk stacks
+    // splat renderer: fixed-point accumulator and RGBA staging, sized for
+    // render_pixels_cap pixels (allocated at the first gcs_render_frame)
+    unsigned long long* render_acc = nullptr;
+    uint8_t* render_rgba = nullptr;
+    int64_t render_pixels_cap = 0;
     size_t walk_stack_entries = 0;
     int32_t group_width = 32;              // targets per walk group (<= 32)
     size_t groups_cap = 0;
@@ -176,7 +182,7 @@ void free_all(gcs_ctx* c) {
                     c->idx[0], c->idx[1], c->tr, c->bd, c->wn, c->com64, c->leaf_parent, c->seg_off,
                     c->seg_id, c->groups, c->chunks, c->seg_bounds, c->staging, c->pb_staging,
                     c->scratch, c->status, c->diag, c->targets, c->direct_out, c->counts,
-                    c->walk_stack};
+                    c->walk_stack, c->render_acc, c->render_rgba};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }
@@ -955,6 +961,126 @@ int gcs_direct_accels_fp64(gcs_ctx* c, const gcs_params* p, int32_t segment,
                                 cudaMemcpyDeviceToHost, c->stream));
     GCS_CUDA(c, cudaStreamSynchronize(c->stream));
     return GCS_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// headless point-splat renderer (renderer.cpp:97-148, 202-204, 248, 262-263)
+// ---------------------------------------------------------------------------
+extern "C" {
+
+void gcs_camera_reference(gcs_camera* cam) {
+    if (!cam) return;
+    const float pos[3] = {0.0f, 150.0f, 600.0f}, front[3] = {0.0f, -0.2f, -1.0f}, up[3] = {0.0f, 1.0f, 0.0f};
+    for (int k = 0; k < 3; ++k) {
+        cam->pos[k] = pos[k];
+        cam->front[k] = front[k];
+        cam->up[k] = up[k];
+    }
+    cam->fovy_deg = 45.0f;
+    cam->z_near = 0.1f;
+    cam->z_far = 5000.0f;
+}
+
+// View = lookAt(eye, eye + front, up): rows s, u, -f (s = normalize(f x up),
+// u = s x f, f = normalize(front)) with translations -s.eye, -u.eye, f.eye.
+// Proj = perspective(fovy, aspect, near, far), OpenGL clip depth [-1, 1].
+// Formed in double, stored as float.
+int gcs_camera_matrices(const gcs_camera* cam, int32_t width, int32_t height, float view[16], float proj[16]) {
+    if (!cam || !view || !proj || width < 1 || height < 1) return GCS_ERR_ARG;
+    if (!(cam->fovy_deg > 0.0f && cam->fovy_deg < 180.0f) || !(cam->z_near > 0.0f) ||
+        !(cam->z_far > cam->z_near))
+        return GCS_ERR_ARG;
+    double f[3] = {cam->front[0], cam->front[1], cam->front[2]};
+    const double fl = std::sqrt(f[0] * f[0] + f[1] * f[1] + f[2] * f[2]);
+    if (!(fl > 0.0)) return GCS_ERR_ARG;
+    for (double& x : f) x /= fl;
+    const double up[3] = {cam->up[0], cam->up[1], cam->up[2]};
+    double sv[3] = {f[1] * up[2] - f[2] * up[1], f[2] * up[0] - f[0] * up[2], f[0] * up[1] - f[1] * up[0]};
+    const double sl = std::sqrt(sv[0] * sv[0] + sv[1] * sv[1] + sv[2] * sv[2]);
+    if (!(sl > 0.0)) return GCS_ERR_ARG;  // up parallel to the view direction
+    for (double& x : sv) x /= sl;
+    const double u[3] = {sv[1] * f[2] - sv[2] * f[1], sv[2] * f[0] - sv[0] * f[2], sv[0] * f[1] - sv[1] * f[0]};
+    const double e[3] = {cam->pos[0], cam->pos[1], cam->pos[2]};
+    const double V[16] = {sv[0], sv[1], sv[2], -(sv[0] * e[0] + sv[1] * e[1] + sv[2] * e[2]),
+                          u[0],  u[1],  u[2],  -(u[0] * e[0] + u[1] * e[1] + u[2] * e[2]),
+                          -f[0], -f[1], -f[2], (f[0] * e[0] + f[1] * e[1] + f[2] * e[2]),
+                          0.0,   0.0,   0.0,   1.0};
+    const double t = std::tan(0.5 * (double)cam->fovy_deg * 3.14159265358979323846 / 180.0);
+    const double aspect = (double)width / (double)height;
+    const double n = cam->z_near, fa = cam->z_far;
+    const double P[16] = {1.0 / (aspect * t), 0.0, 0.0, 0.0,
+                          0.0, 1.0 / t, 0.0, 0.0,
+                          0.0, 0.0, -(fa + n) / (fa - n), -2.0 * fa * n / (fa - n),
+                          0.0, 0.0, -1.0, 0.0};
+    for (int k = 0; k < 16; ++k) {
+        view[k] = (float)V[k];
+        proj[k] = (float)P[k];
+    }
+    return GCS_OK;
+}
+
+int gcs_render_frame(gcs_ctx* c, const gcs_camera* cam, int32_t segment, int32_t width, int32_t height,
+                     uint8_t* rgba, int32_t rgba_on_host) {
+    if (!c || !cam || !rgba || width < 1 || height < 1) return GCS_ERR_ARG;
+    if (segment < -1 || segment >= c->nseg) {
+        c->last_error = "render: segment out of range";
+        return GCS_ERR_ARG;
+    }
+    const int64_t pixels = (int64_t)width * height;
+    if (pixels > ((int64_t)1 << 28)) {
+        c->last_error = "render: frame larger than 2^28 pixels";
+        return GCS_ERR_ARG;
+    }
+    float view[16], proj[16];
+    if (gcs_camera_matrices(cam, width, height, view, proj)) {
+        c->last_error = "render: degenerate camera";
+        return GCS_ERR_ARG;
+    }
+    cudaSetDevice(c->device);
+    if (pixels > c->render_pixels_cap) {
+        // buffers in use by queued frames are released only once those are done
+        GCS_CUDA(c, cudaStreamSynchronize(c->stream));
+        if (c->render_acc) cudaFree(c->render_acc);
+        if (c->render_rgba) cudaFree(c->render_rgba);
+        c->render_acc = nullptr;
+        c->render_rgba = nullptr;
+        c->render_pixels_cap = 0;
+        GCS_CUDA(c, cudaMalloc(reinterpret_cast<void**>(&c->render_acc), sizeof(unsigned long long) * 3 * pixels));
+        GCS_CUDA(c, cudaMalloc(reinterpret_cast<void**>(&c->render_rgba), 4 * (size_t)pixels));
+        c->render_pixels_cap = pixels;
+    }
+    const int64_t first = segment < 0 ? 0 : c->h_seg_off[segment];
+    const int64_t n = segment < 0 ? c->n : c->h_seg_off[segment + 1] - first;
+    GCS_CUDA(c, cudaMemsetAsync(c->render_acc, 0, sizeof(unsigned long long) * 3 * pixels, c->stream));
+    launch_splat_posvel(c->pos[c->cur] + first, c->vel[c->cur] + first, n, view, proj, width, height, c->render_acc,
+                        c->stream);
+    uint8_t* target = rgba_on_host ? c->render_rgba : rgba;
+    launch_resolve(c->render_acc, pixels, target, c->stream);
+    int rc = check_launch(c, "render");
+    if (rc) return rc;
+    if (rgba_on_host) {
+        GCS_CUDA(c, cudaMemcpyAsync(rgba, c->render_rgba, 4 * (size_t)pixels, cudaMemcpyDeviceToHost, c->stream));
+        GCS_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
+    return GCS_OK;
+}
+
+int gcs_render_stars(const Star* stars, int64_t n, const gcs_camera* cam, int32_t width, int32_t height,
+                     uint64_t* accum, uint8_t* rgba, void* stream) {
+    if (n < 0 || (n > 0 && !stars) || !cam || !accum || width < 1 || height < 1) return GCS_ERR_ARG;
+    const int64_t pixels = (int64_t)width * height;
+    if (pixels > ((int64_t)1 << 28)) return GCS_ERR_ARG;
+    if ((reinterpret_cast<uintptr_t>(accum) & 7u) || (reinterpret_cast<uintptr_t>(rgba) & 3u) ||
+        (reinterpret_cast<uintptr_t>(stars) & 15u))
+        return GCS_ERR_ARG;
+    float view[16], proj[16];
+    if (gcs_camera_matrices(cam, width, height, view, proj)) return GCS_ERR_ARG;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    launch_splat_stars(stars, n, view, proj, width, height, reinterpret_cast<unsigned long long*>(accum), st);
+    if (rgba) launch_resolve(reinterpret_cast<const unsigned long long*>(accum), pixels, rgba, st);
+    return cudaGetLastError() == cudaSuccess ? GCS_OK : GCS_ERR_CUDA;
 }
 
 }  // extern "C"

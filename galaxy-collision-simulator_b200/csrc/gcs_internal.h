@@ -157,6 +157,14 @@ void launch_diag(const float4* pos, const float4* vel, const float4* acc, int64_
 // wait for it (the headless interop target of the drop-in API).
 int pack_to_device(gcs_ctx* c, Star* dst);
 
+// Headless point-splat renderer (k_render.cu): fixed-point fragment sums
+// into acc (width*height*3 u64, zeroed by the caller), then RGBA8.
+void launch_splat_posvel(const float4* pos, const float4* vel, int64_t n, const float* view, const float* proj,
+                         int width, int height, unsigned long long* acc, cudaStream_t st);
+void launch_splat_stars(const Star* stars, int64_t n, const float* view, const float* proj, int width, int height,
+                        unsigned long long* acc, cudaStream_t st);
+void launch_resolve(const unsigned long long* acc, int64_t pixels, uint8_t* rgba, cudaStream_t st);
+
 void launch_direct_fp64(const float4* pos, int64_t seg_first, int64_t seg_n, const int64_t* targets,
                         int64_t n_targets, double G, double eps2, double* out, cudaStream_t st);
 

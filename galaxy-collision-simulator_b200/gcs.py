@@ -60,6 +60,13 @@ class CollisionSpec(C.Structure):
                 ("disc_dispersion", C.c_float)]
 
 
+class Camera(C.Structure):
+    """gcs_camera: eye, view direction (looks at pos + front), up, vertical
+    field of view in degrees, near and far planes (renderer.cpp:9-11, 262-263)."""
+    _fields_ = [("pos", C.c_float * 3), ("front", C.c_float * 3), ("up", C.c_float * 3),
+                ("fovy_deg", C.c_float), ("z_near", C.c_float), ("z_far", C.c_float)]
+
+
 class ServerResult(C.Structure):
     _fields_ = [("id", C.c_uint64), ("n", C.c_int64), ("steps", C.c_int32), ("status", C.c_int32),
                 ("queued_ms", C.c_double), ("latency_ms", C.c_double)]
@@ -124,6 +131,10 @@ def lib() -> C.CDLL:
         "gcs_segment_offset": (i64, [P, i32]),
         "gcs_device_bytes": (i64, [P]),
         "gcs_context_bytes": (i64, [i64, i32, i32]),
+        "gcs_camera_reference": (None, [C.POINTER(Camera)]),
+        "gcs_camera_matrices": (C.c_int, [C.POINTER(Camera), i32, i32, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+        "gcs_render_frame": (C.c_int, [P, C.POINTER(Camera), i32, i32, i32, P, i32]),
+        "gcs_render_stars": (C.c_int, [P, i64, C.POINTER(Camera), i32, i32, P, P, P]),
         "gcs_server_create": (C.c_int, [C.POINTER(P), i32, i64, i32, C.c_double, C.POINTER(Params)]),
         "gcs_server_destroy": (None, [P]),
         "gcs_server_context": (P, [P]),
@@ -352,6 +363,13 @@ class Context:
         r = tuple(int(x) for x in out)
         return r if warp_evals else r[:2]
 
+    def render(self, cam: "Camera", width: int, height: int, segment: int = -1) -> np.ndarray:
+        """The headless splat frame of the current particles: (height, width, 4)
+        uint8 RGBA, row 0 at the bottom (GL's framebuffer order)."""
+        out = np.zeros((height, width, 4), np.uint8)
+        self.check(self.L.gcs_render_frame(self._h, C.byref(cam), segment, width, height, _ptr(out), 1))
+        return out
+
     def direct_fp64(self, p: Params, targets, segment: int = 0) -> np.ndarray:
         t = np.ascontiguousarray(targets, dtype=np.int64)
         out = np.zeros((len(t), 3), dtype=np.float64)
@@ -482,3 +500,29 @@ def read_playback(path: str, n: int) -> np.ndarray:
     if len(raw) % n:
         raise GcsError("%s holds %d records, not a whole number of %d-star frames" % (path, len(raw), n))
     return raw.reshape(-1, n)
+
+
+def camera_reference() -> Camera:
+    """The reference's start-up camera (renderer.cpp:9-11, 263)."""
+    cam = Camera()
+    lib().gcs_camera_reference(C.byref(cam))
+    return cam
+
+
+def camera_matrices(cam: Camera, width: int, height: int):
+    """(view, proj) 4x4 float32 row-major matrices the renderer uses."""
+    v = np.zeros(16, np.float32)
+    pm = np.zeros(16, np.float32)
+    rc = lib().gcs_camera_matrices(C.byref(cam), width, height, v.ctypes.data_as(C.POINTER(C.c_float)),
+                                   pm.ctypes.data_as(C.POINTER(C.c_float)))
+    if rc != OK:
+        raise GcsError("gcs_camera_matrices: status %d" % rc)
+    return v.reshape(4, 4), pm.reshape(4, 4)
+
+
+def write_ppm(path: str, rgba: np.ndarray) -> None:
+    """Write an RGBA frame (row 0 at the bottom) as a binary PPM image (top row first)."""
+    h, w = rgba.shape[:2]
+    with open(path, "wb") as f:
+        f.write(b"P6\n%d %d\n255\n" % (w, h))
+        f.write(np.ascontiguousarray(rgba[::-1, :, :3]).tobytes())

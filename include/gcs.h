@@ -291,6 +291,56 @@ int64_t gcs_device_bytes(const gcs_ctx* ctx);
  * (nothing is allocated); a negative status on bad arguments or device. */
 int64_t gcs_context_bytes(int64_t capacity, int32_t max_segments, int32_t device);
 
+/* ---- headless point-splat renderer ------------------------------------------
+ * The reference draws every Star as one GL point (renderer.cpp:97-148,
+ * vertex attributes 226-233): the
+ * vertex shader transforms it by view and projection and sizes it by its
+ * view-space distance d (dark matter, type 1: clamp(2500/d, 1, 6) pixels;
+ * stars: clamp(1000/d, 1, 3)); the fragment shader gives each pixel of the
+ * point's square whose centre lies at normalised radius r <= 1 an alpha of
+ * exp(-3 r^2), times 0.03 with colour (0.4, 0, 0.8) for dark matter and
+ * times 0.15 with the Star's own rgb/255 otherwise; fragments are added to
+ * the framebuffer with glBlendFunc(GL_SRC_ALPHA, GL_ONE) (renderer.cpp:
+ * 202-204) over the clear colour (0.01, 0.01, 0.02, 1) (renderer.cpp:248).
+ * There is no graphics stack here, so the same arithmetic runs as a CUDA
+ * splat: fragments are summed in 64-bit fixed point (2^-24 units per channel,
+ * so a frame does not depend on fragment order) and resolved once to RGBA8
+ * (round to nearest, clamped), row 0 at the bottom as in GL's default
+ * framebuffer.  Points whose centre lies outside the clip volume are culled;
+ * fragments outside the viewport are dropped. */
+typedef struct gcs_camera {
+    float pos[3];       /* eye (renderer.cpp:9) */
+    float front[3];     /* looks at pos + front (renderer.cpp:10, 262) */
+    float up[3];        /* renderer.cpp:11 */
+    float fovy_deg;     /* vertical field of view, degrees (renderer.cpp:263: 45) */
+    float z_near;       /* renderer.cpp:263: 0.1 */
+    float z_far;        /* renderer.cpp:263: 5000 */
+} gcs_camera;
+/* The reference's start-up camera: eye (0, 150, 600), front (0, -0.2, -1),
+ * up (0, 1, 0), 45 degrees, near 0.1, far 5000. */
+void gcs_camera_reference(gcs_camera* cam);
+/* The 4x4 view and projection matrices (row-major, applied to column
+ * vectors) the renderer uses for cam at width x height: glm::lookAt(pos,
+ * pos + front, up) and glm::perspective(fovy, width/height, near, far). */
+int gcs_camera_matrices(const gcs_camera* cam, int32_t width, int32_t height, float view[16],
+                        float proj[16]);
+/* Render the context's current particles of `segment` (-1: every segment)
+ * into rgba (width*height*4 bytes; host memory when rgba_on_host, else
+ * device memory), on the context's stream.  The context keeps a fixed-point
+ * accumulator of width*height*24 bytes, allocated at the first call and
+ * grown when a larger frame is asked for.  A host target synchronises the
+ * stream; a device target does not. */
+int gcs_render_frame(gcs_ctx* ctx, const gcs_camera* cam, int32_t segment, int32_t width,
+                     int32_t height, uint8_t* rgba, int32_t rgba_on_host);
+/* Render n device Stars (for example gcs_dropin_device_stars()) on `stream`
+ * (NULL: the default stream), asynchronously: fragments are added to the
+ * caller's device accumulator accum (width*height*3 uint64, 2^-24 units per
+ * channel, pixel-major r, g, b; zero it before a new frame) and, unless rgba
+ * is NULL, the frame is resolved into the device buffer rgba.  stars must be
+ * 16-byte aligned, accum 8-byte and rgba 4-byte aligned. */
+int gcs_render_stars(const Star* stars, int64_t n, const gcs_camera* cam, int32_t width,
+                     int32_t height, uint64_t* accum, uint8_t* rgba, void* stream);
+
 /* ---- serving ---------------------------------------------------------------
  * Continuous batching of independent collision scenarios on one device (no
  * counterpart in the reference, whose engine holds one simulation in

@@ -414,3 +414,82 @@ void gcs_oracle_step(int n, float* xyzm, float* vel4, int use_bounds, float lo, 
     free(idx);
     free(tmp);
 }
+
+/* ---- headless point-splat renderer --------------------------------------
+ * The reference's GL point pipeline restated on the CPU, in the operation
+ * order of the CUDA splat kernel: vertex shader renderer.cpp:106-122 (view,
+ * projection, size by view-space distance), fragment shader
+ * renderer.cpp:130-147 (r^2 from gl_PointCoord, exp(-3 r^2), colour and
+ * alpha by type), additive blend renderer.cpp:203 over the clear colour
+ * renderer.cpp:248.  Fragments are added to acc in 2^-24 units per
+ * channel. */
+static float row_dot3(const float* m, int r, float x, float y, float z) {
+    return fmaf(m[4 * r + 0], x, fmaf(m[4 * r + 1], y, fmaf(m[4 * r + 2], z, m[4 * r + 3])));
+}
+static float row_dot4(const float* m, int r, float x, float y, float z, float w) {
+    return fmaf(m[4 * r + 0], x, fmaf(m[4 * r + 1], y, fmaf(m[4 * r + 2], z, m[4 * r + 3] * w)));
+}
+
+void gcs_oracle_render(const Star* stars, int64_t n, const float view[16], const float proj[16], int width,
+                       int height, uint64_t* acc, uint8_t* rgba) {
+    const float W = (float)width, H = (float)height;
+    for (int64_t i = 0; i < n; ++i) {
+        const Star* s = stars + i;
+        const float vx = row_dot3(view, 0, s->x, s->y, s->z);
+        const float vy = row_dot3(view, 1, s->x, s->y, s->z);
+        const float vz = row_dot3(view, 2, s->x, s->y, s->z);
+        const float vw = row_dot3(view, 3, s->x, s->y, s->z);
+        const float dist = sqrtf(fmaf(vz, vz, fmaf(vy, vy, vx * vx)));
+        const int dm = s->type == 1;
+        const float size = dm ? fminf(fmaxf(2500.0f / dist, 1.0f), 6.0f) : fminf(fmaxf(1000.0f / dist, 1.0f), 3.0f);
+        const float cx = row_dot4(proj, 0, vx, vy, vz, vw);
+        const float cy = row_dot4(proj, 1, vx, vy, vz, vw);
+        const float cz = row_dot4(proj, 2, vx, vy, vz, vw);
+        const float cw = row_dot4(proj, 3, vx, vy, vz, vw);
+        if (!(cw > 0.0f && fabsf(cx) <= cw && fabsf(cy) <= cw && fabsf(cz) <= cw)) continue;
+        const float xw = fmaf(cx / cw, 0.5f * W, 0.5f * W);
+        const float yw = fmaf(cy / cw, 0.5f * H, 0.5f * H);
+        const float half = size * 0.5f;
+        int i0 = (int)ceilf((xw - half) - 0.5f), i1 = (int)ceilf((xw + half) - 0.5f) - 1;
+        int j0 = (int)ceilf((yw - half) - 0.5f), j1 = (int)ceilf((yw + half) - 0.5f) - 1;
+        if (i0 < 0) i0 = 0;
+        if (j0 < 0) j0 = 0;
+        if (i1 > width - 1) i1 = width - 1;
+        if (j1 > height - 1) j1 = height - 1;
+        float cr, cg, cb, amul;
+        if (dm) {
+            cr = 0.4f;
+            cg = 0.0f;
+            cb = 0.8f;
+            amul = 0.03f;
+        } else {
+            cr = (float)s->r / 255.0f;
+            cg = (float)s->g / 255.0f;
+            cb = (float)s->b / 255.0f;
+            amul = 0.15f;
+        }
+        for (int pj = j0; pj <= j1; ++pj) {
+            const float py = (2.0f * (((float)pj + 0.5f) - yw)) / size;
+            for (int pi = i0; pi <= i1; ++pi) {
+                const float px = (2.0f * (((float)pi + 0.5f) - xw)) / size;
+                const float r2 = fmaf(py, py, px * px);
+                if (r2 > 1.0f) continue;
+                const float a = expf(-r2 * 3.0f) * amul;
+                uint64_t* p = acc + 3 * ((size_t)pj * width + pi);
+                p[0] += (uint64_t)llrintf((cr * a) * 16777216.0f);
+                p[1] += (uint64_t)llrintf((cg * a) * 16777216.0f);
+                p[2] += (uint64_t)llrintf((cb * a) * 16777216.0f);
+            }
+        }
+    }
+    if (!rgba) return;
+    const double clear[3] = {(double)0.01f, (double)0.01f, (double)0.02f};
+    for (int64_t p = 0; p < (int64_t)width * height; ++p) {
+        for (int k = 0; k < 3; ++k) {
+            double v = clear[k] + (double)acc[3 * p + k] * (1.0 / 16777216.0);
+            if (v > 1.0) v = 1.0;
+            rgba[4 * p + k] = (uint8_t)nearbyint(v * 255.0);
+        }
+        rgba[4 * p + 3] = 255;
+    }
+}

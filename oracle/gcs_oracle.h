@@ -70,6 +70,14 @@ void gcs_oracle_step(int n, float* xyzm, float* vel4, int use_bounds, float lo, 
                      float eps2, float theta, int leaf_size, float dt, int recolor, int com_fp64,
                      float* acc, BvhNodeTraverse* nodes);
 
+/* Headless point-splat renderer (renderer.cpp:97-148, 203, 248): every
+ * Star as a GL point through view and proj (row-major 4x4, column vectors),
+ * fragments added to acc (width*height*3, 2^-24 units per channel, zeroed
+ * by the caller); rgba (may be NULL) gets the resolved RGBA8 frame, row 0 at
+ * the bottom. */
+void gcs_oracle_render(const Star* stars, int64_t n, const float view[16], const float proj[16], int width,
+                       int height, uint64_t* acc, uint8_t* rgba);
+
 #ifdef __cplusplus
 }
 #endif

@@ -46,6 +46,7 @@ def lib() -> C.CDLL:
             "gcs_oracle_aggregate": (None, [C.c_int, _P, _P, _P, C.c_int]),
             "gcs_oracle_walk": (None, [C.c_int, _P, _P, _f32, _f32, _f32, C.c_int, _P, _P]),
             "gcs_oracle_integrate": (None, [_i64, _P, _P, _P, _f32, C.c_int]),
+            "gcs_oracle_render": (None, [_P, _i64, _P, _P, C.c_int, C.c_int, _P, _P]),
             "gcs_oracle_direct_fp64": (None, [_i64, _P, _P, _i64, _f64, _f64, _P]),
             "gcs_oracle_step": (None, [C.c_int, _P, _P, C.c_int, _f32, _f32, _f32, _f32, _f32, C.c_int,
                                        _f32, C.c_int, C.c_int, _P, _P]),
@@ -150,6 +151,18 @@ def step(xyzm, vel4, G, eps2, theta, leaf_size, dt, bounds_lohi=None, recolor=Tr
     lib().gcs_oracle_step(n, _ptr(x), _ptr(v), int(use), lo, hi, G, eps2, theta, leaf_size, dt, int(recolor),
                           int(com_fp64), _ptr(acc), _ptr(nodes))
     return x, v, acc, nodes[: n - 1]
+
+
+def render(stars: np.ndarray, view: np.ndarray, proj: np.ndarray, width: int, height: int):
+    """CPU restatement of the splat renderer -> (acc uint64 [h, w, 3], rgba uint8 [h, w, 4])."""
+    st = np.ascontiguousarray(stars)
+    assert st.dtype.itemsize == 32
+    v = f32(np.asarray(view).ravel())
+    p = f32(np.asarray(proj).ravel())
+    acc = np.zeros((height, width, 3), np.uint64)
+    rgba = np.zeros((height, width, 4), np.uint8)
+    lib().gcs_oracle_render(_ptr(st), len(st), _ptr(v), _ptr(p), width, height, _ptr(acc), _ptr(rgba))
+    return acc, rgba
 
 
 # ---------------------------------------------------------------------------
