@@ -75,7 +75,7 @@ struct gcs_ctx {
     uint8_t* render_rgba = nullptr;
     int64_t render_pixels_cap = 0;
     size_t walk_stack_entries = 0;
-    int32_t group_width = 32;              // targets per walk group (<= 32)
+    int32_t group_width = 32;              // targets per walk group (<= 64; two per lane above 32)
     size_t groups_cap = 0;
     bool count_walk = false;
 
@@ -315,7 +315,7 @@ static int run_stage(gcs_ctx* c, const gcs_params* p, int stage) {
                 c->wn_G = wnp.G;
                 c->wn_L = wnp.leaf_size;
             }
-            launch_walk(L, wp, c->pos[c->cur], c->wn, c->groups, c->n_groups, c->acc,
+            launch_walk(L, wp, c->pos[c->cur], c->wn, c->groups, c->n_groups, c->group_width > 32 ? 2 : 1, c->acc,
                         scratch_at<uint32_t>(c, sl.walk_q), c->status, p->walk_blocks_per_sm, c->sm_count,
                         c->count_walk ? c->counts : nullptr, c->walk_stack, c->walk_stack_entries, st);
             return check_launch(c, "walk");
@@ -882,7 +882,7 @@ int gcs_autotune(gcs_ctx* c, gcs_params* p, double* best_walk_ms) {
     cudaEvent_t e0, e1;
     GCS_CUDA(c, cudaEventCreate(&e0));
     GCS_CUDA(c, cudaEventCreate(&e1));
-    const int widths[] = {32, 16};
+    const int widths[] = {64, 32, 16};
     const int leaves[] = {1, 2, 4, 8, 16, 32};
     const int batches[] = {16, 32, 64};
     const int occupancy[] = {0, 4};

@@ -28,9 +28,9 @@ constexpr int kMaxPasses = 10;         // + up to two segment-id digits
 constexpr int kSortThreads = 256;
 constexpr int kSortItems = 16;
 constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys per tile
-constexpr int kGroupSize = 32;         // walk targets per warp group
+constexpr int kGroupSize = 64;         // walk targets per warp group (two per lane above 32)
 
-// Work unit of the walk: up to 32 consecutive sorted particles of one segment.
+// Work unit of the walk: up to kGroupSize consecutive sorted particles of one segment.
 struct WalkGroup {
     int32_t start;
     int32_t count;
@@ -136,12 +136,13 @@ void launch_walk_nodes(const Layout& L, const BvhNodeTraverse* tr, WalkNodeParam
 // level, so 8192 covers batch 64 on trees 128 levels deep.
 constexpr int kWalkGlobalStack = 8192;
 constexpr int kWalkMaxBatch = 64;  // nodes popped per walk round
+// targets_per_lane: 1 for groups of <= 32 targets, 2 for groups of <= 64.
 void launch_walk(const Layout& L, const WalkParams& wp, const float4* pos,
-                 const WalkNode* wn, const WalkGroup* groups, int n_groups,
+                 const WalkNode* wn, const WalkGroup* groups, int n_groups, int targets_per_lane,
                  float4* acc, uint32_t* queue, uint32_t* status, int blocks_per_sm,
                  int sm_count, unsigned long long* counts, int2* gstack, size_t gstack_entries,
                  cudaStream_t st);
-int walk_max_blocks_per_sm(int batch, int with_potential);
+int walk_max_blocks_per_sm(int batch, int with_potential, int targets_per_lane);
 // Persistent walk grid (blocks) for n_groups groups, and the global stack
 // entries that grid needs.
 int64_t walk_grid_blocks(int n_groups, int blocks_per_sm, int sm_count, int with_potential);

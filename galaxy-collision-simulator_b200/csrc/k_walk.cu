@@ -13,32 +13,35 @@
 // With theta = 1 and L = 1 every target sees exactly the reference's set of
 // terms; only the order of the FP32 sums differs.
 //
-// Execution: a persistent grid of warps pulls groups of <= 32 consecutive
-// (Morton-adjacent) targets of one segment from a global work queue.  The
-// warp walks the tree once for its group with one stack; each stack entry
-// carries the mask of lanes that still need that subtree, and each lane
-// takes its own opening decision, so the group walk is the union of the 32
-// per-target walks with no change to any target's terms.  Nodes are read
+// Execution: a persistent grid of warps pulls groups of <= 32*T consecutive
+// (Morton-adjacent) targets of one segment from a global work queue; lane l
+// holds targets l and l+32 (T = 2) of its group.  The warp walks the tree once
+// for its group with one stack; each stack entry carries, for each of the T
+// target slots, the mask of lanes that still need that subtree, and each
+// target takes its own opening decision, so the group walk is the union of
+// the per-target walks with no change to any target's terms.  Nodes are read
 // from walk records (WalkNode: centre of mass and G*mass, width^2, and the
 // children or the bucket range for the step's leaf size), which the
 // aggregation writes beside the traverse records.  Each round:
 //   1. up to `batch` (<= 32*H) entries are popped; lane k fetches the
 //      records of nodes k and k+32 (two 16-byte loads each);
 //   2. each node is classified against the group's bounding box with a
-//      2^-16 relative margin: "take" if every lane of the box must accept
-//      it, "open" if every lane must open it, else "mixed" (the margin is far
-//      above the few-ulp rounding of any lane's own d2, so a class never
-//      contradicts a lane's own test);
-//   3. take nodes whose mask holds every live lane go through a monopole
-//      loop without lane masks, other take nodes through a masked one, mixed
-//      nodes through the per-lane opening test (a predicated monopole and a
-//      ballot of opening lanes); open nodes skip evaluation altogether;
+//      2^-16 relative margin: "take" if every target of the box must accept
+//      it, "open" if every target must open it, else "mixed" (the margin is
+//      far above the few-ulp rounding of any target's own d2, so a class
+//      never contradicts a target's own test);
+//   3. take nodes whose masks hold every live target go through a monopole
+//      loop without masks, other take nodes through a masked one, mixed
+//      nodes through the per-target opening test (a predicated monopole and
+//      a ballot of opening lanes per target slot); open nodes skip
+//      evaluation altogether.  Every node loaded from shared memory is
+//      evaluated for the lane's T targets;
 //   4. in parallel, each lane pushes its nodes' internal children and
 //      appends their particle sources (leaf children, or the whole range of
 //      a small node) at offsets from one warp prefix scan;
 //   5. particle sources accumulate in a per-warp list; when it fills, the
 //      lanes fetch up to 64 source records in parallel into shared memory and
-//      every lane sums them.
+//      every lane sums them for its targets.
 // The stack's top lives in shared memory; when it passes a threshold its
 // bottom is spilled to a per-warp region of global memory (L2) and read back
 // when the top runs low, so batches are never throttled and the logical
@@ -66,40 +69,67 @@ constexpr uint32_t kFull = 0xFFFFFFFFu;
 
 // Classes of a batch node against the group's bounding box.
 constexpr int kClassNone = 0;      // lane holds no node
-constexpr int kClassTake = 1;      // every lane of the group accepts it
-constexpr int kClassOpen = 2;      // every lane of the group opens it
-constexpr int kClassMixed = 3;     // lanes decide one by one
-constexpr int kClassTakeFull = 4;  // kClassTake, and every live lane is in its mask
+constexpr int kClassTake = 1;      // every target of the group accepts it
+constexpr int kClassOpen = 2;      // every target of the group opens it
+constexpr int kClassMixed = 3;     // targets decide one by one
+constexpr int kClassTakeFull = 4;  // kClassTake, and every live target is in its masks
 constexpr float kBoxLo = 1.0f - 1.0f / 65536.0f;
 constexpr float kBoxHi = 1.0f + 1.0f / 65536.0f;
 
-// Per-warp shared memory for H nodes per lane per round.  Nodes and sources
-// to evaluate are stored in pairs (slot 2q and 2q+1 side by side), so that
-// one packed FP32 instruction (sm_100 f32x2) evaluates two of them: take
-// nodes fill slots [0, n_take), mixed nodes start at the next even slot, and
-// an odd list is padded with an empty entry (mass 0 at 1e30 in every
-// coordinate, lane mask 0).
-template <int H>
+// Stack entry: node index and one lane mask per target slot.
+template <int T>
+struct EntryOf;
+template <>
+struct EntryOf<1> {
+    using type = int2;
+};
+template <>
+struct EntryOf<2> {
+    using type = int4;
+};
+__device__ __forceinline__ int2 make_entry(int node, const uint32_t (&m)[1]) { return make_int2(node, (int)m[0]); }
+__device__ __forceinline__ int4 make_entry(int node, const uint32_t (&m)[2]) {
+    return make_int4(node, (int)m[0], (int)m[1], 0);
+}
+__device__ __forceinline__ void entry_masks(int2 e, uint32_t (&m)[1]) { m[0] = (uint32_t)e.y; }
+__device__ __forceinline__ void entry_masks(int4 e, uint32_t (&m)[2]) {
+    m[0] = (uint32_t)e.y;
+    m[1] = (uint32_t)e.z;
+}
+
+// Per-warp shared memory for H nodes per lane per round and T targets per
+// lane.  Nodes and sources to evaluate are stored in pairs (slot 2q and 2q+1
+// side by side), so that one packed FP32 instruction (sm_100 f32x2) evaluates
+// two of them: full-mask take nodes fill slots [0, n_full), other take nodes
+// and mixed nodes each start at the next even slot, and an odd list is padded
+// with an empty entry (mass 0 at 1e30 in every coordinate, lane masks 0).
+template <int H, int T>
 struct WarpSmem {
+    using Entry = typename EntryOf<T>::type;
     static constexpr int kBatch = 32 * H;
-    static constexpr int kPairs = kBatch / 2 + 2;                  // three padded lists
-    static constexpr int kStackCap = 256 + 64 * H;                 // stack entries
-    static constexpr int kSpillAbove = kStackCap - 2 * kBatch;     // a round pushes <= 2*batch
-    int2 stk[kStackCap];          // node, lane mask
-    float4 pxy[kPairs];           // x0 x1 y0 y1 of the centres of mass of slots 2q, 2q+1
-    float4 pzm[kPairs];           // z0 z1 Gm0 Gm1
-    float2 pw2[kPairs];           // width^2 of both slots
-    uint2 pmask[kPairs];          // lane masks of both slots
-    uint2 pnopen[kPairs];         // opening lanes of both slots (mixed nodes)
-    float4 sxy[kSrcCap / 2];      // particle sources in pairs: x0 x1 y0 y1
-    float4 szm[kSrcCap / 2];      // z0 z1 Gm0 Gm1
-    uint2 smask[kSrcCap / 2];     // lane masks
-    int2 srcm[kSrcCap];           // particle, lane mask (the list before its fetch)
+    static constexpr int kPairs = kBatch / 2 + 2;  // three padded lists
+    // A round starts with top <= kSpillAbove (or < kBatch before a refill of
+    // <= kSpillCount) and pushes <= 2 * batch; one spill of kSpillCount
+    // brings top back to <= kSpillAbove.
+    static constexpr int kStackCap = T == 1 ? 256 + 64 * H : kSpillCount + 2 * kBatch + 32;
+    static constexpr int kSpillAbove = kStackCap - 2 * kBatch;
+    static_assert(kSpillAbove >= kSpillCount && kBatch <= kSpillCount, "stack sizing");
+    static_assert(2 * kBatch + kSpillCount - 1 <= kStackCap, "refill then push must fit");
+    Entry stk[kStackCap];           // node, lane masks
+    float4 pxy[kPairs];             // x0 x1 y0 y1 of the centres of mass of slots 2q, 2q+1
+    float4 pzm[kPairs];             // z0 z1 Gm0 Gm1
+    float2 pw2[kPairs];             // width^2 of both slots
+    uint2 pmask[T][kPairs];         // lane masks of both slots, per target slot
+    uint2 pnopen[T][kPairs];        // opening lanes of both slots (mixed nodes)
+    float4 sxy[kSrcCap / 2];        // particle sources in pairs: x0 x1 y0 y1
+    float4 szm[kSrcCap / 2];        // z0 z1 Gm0 Gm1
+    uint2 smask[T][kSrcCap / 2];    // lane masks
+    int srcp[kSrcCap];              // the list before its fetch: particle
+    uint32_t srcm[T][kSrcCap];      //   and its lane masks
 };
 
-// Store one evaluation entry at pair slot `slot` of a pair-interleaved list.
-__device__ __forceinline__ void put_pair(float4* xy, float4* zm, uint2* mk, int slot, float4 c,
-                                         uint32_t mask) {
+// Store one entry's coordinates at pair slot `slot` of a pair-interleaved list.
+__device__ __forceinline__ void put_pair(float4* xy, float4* zm, int slot, float4 c) {
     const int q = slot >> 1, e = slot & 1;
     float* fxy = reinterpret_cast<float*>(xy + q);
     float* fzm = reinterpret_cast<float*>(zm + q);
@@ -107,31 +137,35 @@ __device__ __forceinline__ void put_pair(float4* xy, float4* zm, uint2* mk, int 
     fxy[2 + e] = c.y;
     fzm[e] = c.z;
     fzm[2 + e] = c.w;
-    reinterpret_cast<uint32_t*>(mk + q)[e] = mask;
+}
+__device__ __forceinline__ void put_mask(uint2* mk, int slot, uint32_t mask) {
+    reinterpret_cast<uint32_t*>(mk + (slot >> 1))[slot & 1] = mask;
 }
 
-// Resident blocks per SM the register budget is set for (H=1: 48 registers
-// a thread, 40 warps; H=2: 64 registers, 32 warps).
-template <int H>
+// Resident blocks per SM the register budget is set for (T=1: H=1 48
+// registers a thread, 40 warps; H=2 64 registers, 32 warps; T=2: 80
+// registers, 24 warps).
+template <int H, int T>
 struct WalkOcc {
-    static constexpr int kMinBlocks = H == 1 ? 5 : 4;
+    static constexpr int kMinBlocks = T == 2 ? 3 : (H == 1 ? 5 : 4);
 };
 
+// Sums of one target: two partial sums per component (even / odd slots).
 struct Accum {
-    float2 ax, ay, az, pot;       // two partial sums per component (even / odd slots)
-    uint32_t n_mono, n_part;      // interaction counts (count mode only)
-    uint32_t w_node, w_src;       // warp-wide node / source evaluations (count mode only)
+    float2 ax, ay, az, pot;
+    uint32_t n_mono, n_part;  // interaction counts (count mode only)
+};
+// Warp-wide counters (count mode only).
+struct WarpCount {
+    uint32_t w_node, w_src;       // warp-wide node / source evaluations
     uint32_t rounds, spills;      // pop rounds, stack spills to global memory
     uint32_t all_open, all_take;  // nodes classified open / take by the box test
 };
 
-// Sum the listed particle sources into every lane whose bit is in the
-// source's mask (leaf rule: skip d2 <= 1.01 eps^2).
-// Two evaluation entries for this lane, packed (sm_100 f32x2): d = c - x and
-// the softened d2 of both, then the terms of the entries whose `use` is
-// set.  Each element is rounded exactly as the scalar forms round it
-// (softened_d2, the hardware 1/sqrt, inv^3, G m inv^3, one FMA per
-// component); each lane keeps two partial sums (even and odd slots).
+// Two evaluation entries for one target, packed (sm_100 f32x2): d = c - x
+// and the softened d2 of both.  Each element is rounded exactly as the
+// scalar forms round it (softened_d2), so opening decisions are the
+// reference's.
 struct PairD {
     float2 dx, dy, dz, d2;
 };
@@ -145,7 +179,7 @@ __device__ __forceinline__ PairD pair_d(float4 xy, float4 zm, float2 npx, float2
     return r;
 }
 
-// pair_d for nodes every lane of the entry accepts: no opening decision
+// pair_d for nodes every target of the entry accepts: no opening decision
 // depends on d2 here, so eps^2 starts the FMA chain (d2 differs from the
 // decision form by rounding only).
 __device__ __forceinline__ PairD pair_d_take(float4 xy, float4 zm, float2 npx, float2 npy, float2 npz, float2 e2) {
@@ -157,6 +191,8 @@ __device__ __forceinline__ PairD pair_d_take(float4 xy, float4 zm, float2 npx, f
     return r;
 }
 
+// Terms of the two entries whose `use` is set: the hardware 1/sqrt, inv^3,
+// G m inv^3, one FMA per component.
 template <bool kPot>
 __device__ __forceinline__ void pair_add(Accum& A, const PairD& d, float4 zm, bool use0, bool use1) {
     const float2 inv = make_float2(rsqrt_approx(d.d2.x), rsqrt_approx(d.d2.y));
@@ -174,69 +210,51 @@ __device__ __forceinline__ void pair_add(Accum& A, const PairD& d, float4 zm, bo
     }
 }
 
-// Sum the listed particle sources into every lane whose bit is in the
-// source's mask (leaf rule: skip d2 <= 1.01 eps^2).
-// One packed evaluation of two entries for this lane: terms of the entries
-// whose `use` is set are added to the two partial sums.  Each term is
-// rounded exactly as the scalar form (d = c - x, softened_d2, the hardware
-// 1/sqrt, inv^3, G m inv^3, one FMA per component).
-template <bool kPot>
-__device__ __forceinline__ void add_pair(Accum& A, float4 xy, float4 zm, float2 npx, float2 npy, float2 npz,
-                                         float2 e2, bool use0, bool use1, float2& d2_out, bool& d2_ready) {
-    (void)d2_ready;
-    const float2 dx = __fadd2_rn(make_float2(xy.x, xy.y), npx);
-    const float2 dy = __fadd2_rn(make_float2(xy.z, xy.w), npy);
-    const float2 dz = __fadd2_rn(make_float2(zm.x, zm.y), npz);
-    const float2 d2 = softened_d2_x2(dx, dy, dz, e2);
-    d2_out = d2;
-    const float2 inv = make_float2(rsqrt_approx(d2.x), rsqrt_approx(d2.y));
-    const float2 inv3 = __fmul2_rn(__fmul2_rn(inv, inv), inv);
-    float2 f = __fmul2_rn(make_float2(zm.z, zm.w), inv3);
-    f.x = use0 ? f.x : 0.0f;
-    f.y = use1 ? f.y : 0.0f;
-    A.ax = __ffma2_rn(dx, f, A.ax);
-    A.ay = __ffma2_rn(dy, f, A.ay);
-    A.az = __ffma2_rn(dz, f, A.az);
-    if (kPot) {
-        const float2 t = __ffma2_rn(make_float2(-zm.z, -zm.w), inv, A.pot);
-        A.pot.x = use0 ? t.x : A.pot.x;
-        A.pot.y = use1 ? t.y : A.pot.y;
-    }
-}
+// The lane's targets: position as packed negatives (for d = c - x).
+template <int T>
+struct Targets {
+    float2 npx[T], npy[T], npz[T];
+};
 
-// Sum the listed particle sources into every lane whose bit is in the
-// source's mask (leaf rule: skip d2 <= 1.01 eps^2).
-template <int H, bool kPot, bool kCount>
-__device__ __forceinline__ void flush_sources(WarpSmem<H>& W, int nsrc, int lane, uint32_t lane_bit,
-                                              const float4* __restrict__ pos, float G, float4 p,
-                                              float eps2, float leaf_thr, Accum& A) {
+// Sum the listed particle sources into every target whose lane bit is in
+// the source's mask for its slot (leaf rule: skip d2 <= 1.01 eps^2).
+template <int H, int T, bool kPot, bool kCount>
+__device__ __forceinline__ void flush_sources(WarpSmem<H, T>& W, int nsrc, int lane, uint32_t lane_bit,
+                                              const float4* __restrict__ pos, float G, const Targets<T>& X,
+                                              float2 e2, float leaf_thr, Accum (&A)[T], WarpCount& WC) {
     __syncwarp();
     const int padded = (nsrc + 1) & ~1;
     for (int e = lane; e < padded; e += 32) {
         float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
-        uint32_t mask = 0u;
+        uint32_t m[T];
+#pragma unroll
+        for (int t = 0; t < T; ++t) m[t] = 0u;
         if (e < nsrc) {
-            const int2 sm = W.srcm[e];
-            q = __ldg(pos + sm.x);
+            q = __ldg(pos + W.srcp[e]);
             q.w = __fmul_rn(G, q.w);
-            mask = (uint32_t)sm.y;
+#pragma unroll
+            for (int t = 0; t < T; ++t) m[t] = W.srcm[t][e];
         }
-        put_pair(W.sxy, W.szm, W.smask, e, q, mask);
+        put_pair(W.sxy, W.szm, e, q);
+#pragma unroll
+        for (int t = 0; t < T; ++t) put_mask(W.smask[t], e, m[t]);
     }
     __syncwarp();
-    const float2 npx = make_float2(-p.x, -p.x), npy = make_float2(-p.y, -p.y), npz = make_float2(-p.z, -p.z);
-    const float2 e2 = make_float2(eps2, eps2);
 #pragma unroll 2
     for (int q = 0; q < (padded >> 1); ++q) {
         const float4 zm = W.szm[q];
-        const uint2 mk = W.smask[q];
-        const PairD d = pair_d(W.sxy[q], zm, npx, npy, npz, e2);
-        const bool use0 = (mk.x & lane_bit) && (d.d2.x > leaf_thr);
-        const bool use1 = (mk.y & lane_bit) && (d.d2.y > leaf_thr);
-        pair_add<kPot>(A, d, zm, use0, use1);
-        if (kCount) A.n_part += (use0 ? 1u : 0u) + (use1 ? 1u : 0u);
+        const float4 xy = W.sxy[q];
+#pragma unroll
+        for (int t = 0; t < T; ++t) {
+            const uint2 mk = W.smask[t][q];
+            const PairD d = pair_d(xy, zm, X.npx[t], X.npy[t], X.npz[t], e2);
+            const bool use0 = (mk.x & lane_bit) && (d.d2.x > leaf_thr);
+            const bool use1 = (mk.y & lane_bit) && (d.d2.y > leaf_thr);
+            pair_add<kPot>(A[t], d, zm, use0, use1);
+            if (kCount) A[t].n_part += (use0 ? 1u : 0u) + (use1 ? 1u : 0u);
+        }
     }
-    if (kCount) A.w_src += (uint32_t)nsrc;
+    if (kCount) WC.w_src += (uint32_t)nsrc;
     __syncwarp();
 }
 
@@ -250,28 +268,29 @@ __device__ __forceinline__ uint32_t warp_exclusive_scan(uint32_t v, int lane) {
     return x - v;
 }
 
-template <int H, bool kPot, bool kCount>
-__global__ void __launch_bounds__(kWalkThreads, WalkOcc<H>::kMinBlocks)
+template <int H, int T, bool kPot, bool kCount>
+__global__ void __launch_bounds__(kWalkThreads, (WalkOcc<H, T>::kMinBlocks))
 walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
             const WalkNode* __restrict__ wn, const WalkGroup* __restrict__ groups,
             int n_groups, float4* __restrict__ acc, uint32_t* __restrict__ queue,
             uint32_t* __restrict__ status, unsigned long long* __restrict__ counts,
-            int2* __restrict__ gstack, int gstack_cap) {
-    using Smem = WarpSmem<H>;
+            typename EntryOf<T>::type* __restrict__ gstack, int gstack_cap) {
+    using Smem = WarpSmem<H, T>;
+    using Entry = typename Smem::Entry;
     extern __shared__ __align__(16) unsigned char walk_smem[];
     const int warp = threadIdx.x >> 5;
     Smem& W = reinterpret_cast<Smem*>(walk_smem)[warp];
-    int2* const gstk = gstack + ((size_t)blockIdx.x * kWalkWarps + warp) * (size_t)gstack_cap;
+    Entry* const gstk = gstack + ((size_t)blockIdx.x * kWalkWarps + warp) * (size_t)gstack_cap;
     const int lane = threadIdx.x & 31;
     const uint32_t lane_bit = 1u << lane;
     const uint32_t lt = lane_bit - 1u;
     const float G = wp.G, eps2 = wp.eps2, theta2 = wp.theta2;
     const float2 e2 = make_float2(eps2, eps2), th2 = make_float2(theta2, theta2);
     const float leaf_thr = __fmul_rn(eps2, 1.01f);
-    const int batch = wp.batch;
     // box classification thresholds: take iff w^2 < s2min * k_take, open iff
     // w^2 >= s2max * k_open (theta^2 with the 2^-16 relative margin)
     const float k_take = theta2 * kBoxLo, k_open = theta2 * kBoxHi;
+    const int batch = wp.batch;
 
     for (;;) {
         int g = 0;
@@ -279,13 +298,28 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
         g = __shfl_sync(kFull, g, 0);
         if (g >= n_groups) break;
         const WalkGroup grp = groups[g];
-        const bool valid = lane < grp.count;
-        const int t = grp.start + lane;
-        const float4 p = valid ? __ldg(pos + t) : make_float4(0.f, 0.f, 0.f, 0.f);
-        const uint32_t live = __ballot_sync(kFull, valid);
+        bool valid[T];
+        uint32_t live[T];
+        Targets<T> X;
         // bounding box of the group's targets
-        float3 box_lo = valid ? make_float3(p.x, p.y, p.z) : make_float3(INFINITY, INFINITY, INFINITY);
-        float3 box_hi = valid ? make_float3(p.x, p.y, p.z) : make_float3(-INFINITY, -INFINITY, -INFINITY);
+        float3 box_lo = make_float3(INFINITY, INFINITY, INFINITY);
+        float3 box_hi = make_float3(-INFINITY, -INFINITY, -INFINITY);
+        Accum A[T];
+#pragma unroll
+        for (int t = 0; t < T; ++t) {
+            valid[t] = lane + 32 * t < grp.count;
+            const float4 p = valid[t] ? __ldg(pos + grp.start + lane + 32 * t) : make_float4(0.f, 0.f, 0.f, 0.f);
+            live[t] = __ballot_sync(kFull, valid[t]);
+            X.npx[t] = make_float2(-p.x, -p.x);
+            X.npy[t] = make_float2(-p.y, -p.y);
+            X.npz[t] = make_float2(-p.z, -p.z);
+            if (valid[t]) {
+                box_lo = make_float3(fminf(box_lo.x, p.x), fminf(box_lo.y, p.y), fminf(box_lo.z, p.z));
+                box_hi = make_float3(fmaxf(box_hi.x, p.x), fmaxf(box_hi.y, p.y), fmaxf(box_hi.z, p.z));
+            }
+            A[t].ax = A[t].ay = A[t].az = A[t].pot = make_float2(0.f, 0.f);
+            A[t].n_mono = A[t].n_part = 0u;
+        }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             box_lo.x = fminf(box_lo.x, __shfl_xor_sync(kFull, box_lo.x, o));
@@ -298,15 +332,13 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
         const int s = grp.seg;
         const int off = (int)__ldg(L.seg_off + s);
         const int seg_n = (int)__ldg(L.seg_off + s + 1) - off;
-        Accum A;
-        A.ax = A.ay = A.az = A.pot = make_float2(0.f, 0.f);
-        A.n_mono = A.n_part = A.w_node = A.w_src = A.rounds = A.spills = A.all_open = A.all_take = 0u;
-        const float2 npx = make_float2(-p.x, -p.x), npy = make_float2(-p.y, -p.y), npz = make_float2(-p.z, -p.z);
+        WarpCount WC;
+        WC.w_node = WC.w_src = WC.rounds = WC.spills = WC.all_open = WC.all_take = 0u;
         int nsrc = 0;
 
         if (seg_n >= 2) {
             int top = 1, gtop = 0;
-            if (lane == 0) W.stk[0] = make_int2(off - s, (int)live);
+            if (lane == 0) W.stk[0] = make_entry(off - s, live);
             __syncwarp();
             // Each internal node has one parent, so a walk pops it at most
             // once: more pops than internal nodes means a malformed tree.
@@ -315,10 +347,9 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                 // refill the shared top from the global bottom when it runs low
                 if (top < batch && gtop > 0) {
                     const int k = gtop < kSpillCount ? gtop : kSpillCount;
-                    int2 keep[H];
+                    Entry keep[H];
 #pragma unroll
-                    for (int h = 0; h < H; ++h)
-                        keep[h] = lane + 32 * h < top ? W.stk[lane + 32 * h] : make_int2(0, 0);
+                    for (int h = 0; h < H; ++h) keep[h] = lane + 32 * h < top ? W.stk[lane + 32 * h] : Entry{};
                     __syncwarp();
 #pragma unroll
                     for (int h = 0; h < H; ++h)
@@ -337,7 +368,7 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                 top -= b;
                 // 1-2. fetch and classify nodes lane and lane+32
                 int code_a[H], code_b[H], cls[H];
-                uint32_t my_mask[H];
+                uint32_t my_mask[H][T];
                 float4 com[H];
                 float w2[H];
 #pragma unroll
@@ -346,11 +377,12 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                     code_a[h] = 0;
                     code_b[h] = kWalkSkipTag;
                     cls[h] = kClassNone;
-                    my_mask[h] = 0u;
+#pragma unroll
+                    for (int t = 0; t < T; ++t) my_mask[h][t] = 0u;
                     com[h] = make_float4(0.f, 0.f, 0.f, 0.f);
                     w2[h] = 0.0f;
                     if (j < b) {
-                        const int2 e = W.stk[top + j];
+                        const Entry e = W.stk[top + j];
                         const float4* np = reinterpret_cast<const float4*>(wn + e.x);
                         const float4 a = __ldg(np);
                         const int4 k = __ldg(reinterpret_cast<const int4*>(np + 1));
@@ -358,7 +390,10 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                         code_a[h] = k.y;
                         code_b[h] = k.z;
                         com[h] = a;
-                        my_mask[h] = (uint32_t)e.y;
+                        entry_masks(e, my_mask[h]);
+                        bool full = true;
+#pragma unroll
+                        for (int t = 0; t < T; ++t) full = full && my_mask[h][t] == live[t];
                         // squared softened distances from the centre of mass
                         // to the nearest and farthest points of the box
                         float s2min = eps2, s2max = eps2;
@@ -373,15 +408,15 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                                 s2max = fmaf(far, far, s2max);
                             }
                         }
-                        if (w2[h] < s2min * k_take) cls[h] = my_mask[h] == live ? kClassTakeFull : kClassTake;
+                        if (w2[h] < s2min * k_take) cls[h] = full ? kClassTakeFull : kClassTake;
                         else if (w2[h] >= s2max * k_open) cls[h] = kClassOpen;
                         else cls[h] = kClassMixed;
                     }
                 }
                 // compact into three pair-interleaved lists, each starting at
-                // an even slot: take nodes with every live lane in their mask,
-                // other take nodes, mixed nodes; odd lists end with an empty
-                // entry
+                // an even slot: take nodes with every live target in their
+                // masks, other take nodes, mixed nodes; odd lists end with an
+                // empty entry
                 uint32_t bf[H], bt[H], bm[H];
                 int n_full = 0, n_take = 0, n_mixed = 0;
 #pragma unroll
@@ -407,7 +442,9 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                         take_before += __popc(bt[h]);
                         mixed_before += __popc(bm[h]);
                         if (slot[h] >= 0) {
-                            put_pair(W.pxy, W.pzm, W.pmask, slot[h], com[h], my_mask[h]);
+                            put_pair(W.pxy, W.pzm, slot[h], com[h]);
+#pragma unroll
+                            for (int t = 0; t < T; ++t) put_mask(W.pmask[t], slot[h], my_mask[h][t]);
                             reinterpret_cast<float*>(W.pw2 + (slot[h] >> 1))[slot[h] & 1] = w2[h];
                         }
                     }
@@ -416,64 +453,88 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                                   : lane == 1 ? ((n_take & 1) ? take_base + n_take : -1)
                                   : lane == 2 ? ((n_mixed & 1) ? mixed_base + n_mixed : -1) : -1;
                     if (pad >= 0) {
-                        put_pair(W.pxy, W.pzm, W.pmask, pad, empty, 0u);
+                        put_pair(W.pxy, W.pzm, pad, empty);
+#pragma unroll
+                        for (int t = 0; t < T; ++t) put_mask(W.pmask[t], pad, 0u);
                         reinterpret_cast<float*>(W.pw2 + (pad >> 1))[1] = 0.0f;
                     }
                 }
                 __syncwarp();
                 if (kCount) {
-                    A.w_node += (uint32_t)b;
-                    A.rounds += 1u;
-                    A.all_open += (uint32_t)(b - n_full - n_take - n_mixed);
-                    A.all_take += (uint32_t)(n_full + n_take);
+                    WC.w_node += (uint32_t)b;
+                    WC.rounds += 1u;
+                    WC.all_open += (uint32_t)(b - n_full - n_take - n_mixed);
+                    WC.all_take += (uint32_t)(n_full + n_take);
                 }
-                // 3a. nodes every live lane accepts: monopole terms, two
-                // nodes per packed evaluation, no lane masks
+                // 3a. nodes every live target accepts: monopole terms, two
+                // nodes per packed evaluation, no masks
 #pragma unroll 2
                 for (int q = 0; q < (take_base >> 1); ++q) {
                     const float4 zm = W.pzm[q];
-                    const PairD d = pair_d_take(W.pxy[q], zm, npx, npy, npz, e2);
-                    pair_add<kPot>(A, d, zm, true, true);
+                    const float4 xy = W.pxy[q];
+#pragma unroll
+                    for (int t = 0; t < T; ++t) {
+                        const PairD d = pair_d_take(xy, zm, X.npx[t], X.npy[t], X.npz[t], e2);
+                        pair_add<kPot>(A[t], d, zm, true, true);
+                    }
                 }
-                if (kCount && valid) A.n_mono += (uint32_t)n_full;
-                // 3b. nodes accepted by every lane of their mask
+                if (kCount) {
+#pragma unroll
+                    for (int t = 0; t < T; ++t)
+                        if (valid[t]) A[t].n_mono += (uint32_t)n_full;
+                }
+                // 3b. nodes accepted by every target of their masks
 #pragma unroll 2
                 for (int q = take_base >> 1; q < (mixed_base >> 1); ++q) {
                     const float4 zm = W.pzm[q];
-                    const uint2 mk = W.pmask[q];
-                    const PairD d = pair_d_take(W.pxy[q], zm, npx, npy, npz, e2);
-                    const bool use0 = (mk.x & lane_bit) != 0u, use1 = (mk.y & lane_bit) != 0u;
-                    pair_add<kPot>(A, d, zm, use0, use1);
-                    if (kCount) A.n_mono += (use0 ? 1u : 0u) + (use1 ? 1u : 0u);
+                    const float4 xy = W.pxy[q];
+#pragma unroll
+                    for (int t = 0; t < T; ++t) {
+                        const uint2 mk = W.pmask[t][q];
+                        const PairD d = pair_d_take(xy, zm, X.npx[t], X.npy[t], X.npz[t], e2);
+                        const bool use0 = (mk.x & lane_bit) != 0u, use1 = (mk.y & lane_bit) != 0u;
+                        pair_add<kPot>(A[t], d, zm, use0, use1);
+                        if (kCount) A[t].n_mono += (use0 ? 1u : 0u) + (use1 ? 1u : 0u);
+                    }
                 }
-                // 3c. mixed nodes: each lane's own test; lane 0 records the
+                // 3c. mixed nodes: each target's own test; lane 0 records the
                 // ballots of opening lanes for the nodes' owners
                 for (int q = mixed_base >> 1; q < ((mixed_base + n_mixed + 1) >> 1); ++q) {
                     const float4 zm = W.pzm[q];
-                    const uint2 mk = W.pmask[q];
+                    const float4 xy = W.pxy[q];
                     const float2 w2q = W.pw2[q];
-                    const PairD d = pair_d(W.pxy[q], zm, npx, npy, npz, e2);
-                    const float2 lim = __fmul2_rn(d.d2, th2);  // accept_monopole: w^2 < d2 * theta^2
-                    const bool act0 = (mk.x & lane_bit) != 0u, act1 = (mk.y & lane_bit) != 0u;
-                    const bool take0 = w2q.x < lim.x, take1 = w2q.y < lim.y;
-                    pair_add<kPot>(A, d, zm, act0 && take0, act1 && take1);
-                    if (kCount) A.n_mono += (act0 && take0 ? 1u : 0u) + (act1 && take1 ? 1u : 0u);
-                    const uint32_t om0 = __ballot_sync(kFull, act0 && !take0);
-                    const uint32_t om1 = __ballot_sync(kFull, act1 && !take1);
-                    if (lane == 0) W.pnopen[q] = make_uint2(om0, om1);
+#pragma unroll
+                    for (int t = 0; t < T; ++t) {
+                        const uint2 mk = W.pmask[t][q];
+                        const PairD d = pair_d(xy, zm, X.npx[t], X.npy[t], X.npz[t], e2);
+                        const float2 lim = __fmul2_rn(d.d2, th2);  // accept_monopole: w^2 < d2 * theta^2
+                        const bool act0 = (mk.x & lane_bit) != 0u, act1 = (mk.y & lane_bit) != 0u;
+                        const bool take0 = w2q.x < lim.x, take1 = w2q.y < lim.y;
+                        pair_add<kPot>(A[t], d, zm, act0 && take0, act1 && take1);
+                        if (kCount) A[t].n_mono += (act0 && take0 ? 1u : 0u) + (act1 && take1 ? 1u : 0u);
+                        const uint32_t om0 = __ballot_sync(kFull, act0 && !take0);
+                        const uint32_t om1 = __ballot_sync(kFull, act1 && !take1);
+                        if (lane == 0) W.pnopen[t][q] = make_uint2(om0, om1);
+                    }
                 }
                 __syncwarp();
                 // 4. parallel push / append for the opened nodes
-                uint32_t my_open[H];
+                uint32_t my_open[H][T];
                 int n_push[H], n_src[H];
                 int lane_push = 0, lane_src = 0;
 #pragma unroll
                 for (int h = 0; h < H; ++h) {
-                    my_open[h] = cls[h] == kClassOpen ? my_mask[h]
-                               : (cls[h] == kClassMixed ? reinterpret_cast<const uint32_t*>(W.pnopen)[slot[h]] : 0u);
+                    uint32_t any = 0u;
+#pragma unroll
+                    for (int t = 0; t < T; ++t) {
+                        my_open[h][t] = cls[h] == kClassOpen ? my_mask[h][t]
+                                      : (cls[h] == kClassMixed
+                                             ? reinterpret_cast<const uint32_t*>(W.pnopen[t])[slot[h]] : 0u);
+                        any |= my_open[h][t];
+                    }
                     n_push[h] = 0;
                     n_src[h] = 0;
-                    if (my_open[h] != 0u && code_b[h] != kWalkSkipTag) {
+                    if (any != 0u && code_b[h] != kWalkSkipTag) {
                         if (code_b[h] >= kWalkBucketTag) {
                             n_src[h] = code_b[h] - kWalkBucketTag;
                         } else {
@@ -492,8 +553,8 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
 #pragma unroll
                     for (int h = 0; h < H; ++h) {
                         if (n_push[h] > 0) {
-                            if (code_a[h] >= 0) W.stk[at++] = make_int2(code_a[h], (int)my_open[h]);
-                            if (code_b[h] >= 0) W.stk[at++] = make_int2(code_b[h], (int)my_open[h]);
+                            if (code_a[h] >= 0) W.stk[at++] = make_entry(code_a[h], my_open[h]);
+                            if (code_b[h] >= 0) W.stk[at++] = make_entry(code_b[h], my_open[h]);
                         }
                     }
                 }
@@ -505,7 +566,7 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                 const int add = (int)(total & 0xFFFFu);
                 for (int base = 0; base < add;) {
                     if (nsrc == kSrcCap) {
-                        flush_sources<H, kPot, kCount>(W, nsrc, lane, lane_bit, pos, G, p, eps2, leaf_thr, A);
+                        flush_sources<H, T, kPot, kCount>(W, nsrc, lane, lane_bit, pos, G, X, e2, leaf_thr, A, WC);
                         nsrc = 0;
                     }
                     const int window = min(kSrcCap - nsrc, add - base);
@@ -518,7 +579,10 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                             int particle;
                             if (code_b[h] >= kWalkBucketTag) particle = code_a[h] + r;
                             else particle = (r == 0 && code_a[h] < 0) ? ~code_a[h] : ~code_b[h];
-                            W.srcm[nsrc + (j - base)] = make_int2(particle, (int)my_open[h]);
+                            const int at = nsrc + (j - base);
+                            W.srcp[at] = particle;
+#pragma unroll
+                            for (int t = 0; t < T; ++t) W.srcm[t][at] = my_open[h][t];
                         }
                         first += n_src[h];
                     }
@@ -527,7 +591,7 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                 }
                 __syncwarp();
                 if (nsrc >= 32) {
-                    flush_sources<H, kPot, kCount>(W, nsrc, lane, lane_bit, pos, G, p, eps2, leaf_thr, A);
+                    flush_sources<H, T, kPot, kCount>(W, nsrc, lane, lane_bit, pos, G, X, e2, leaf_thr, A, WC);
                     nsrc = 0;
                 }
                 // spill the shared stack's bottom before it can overflow
@@ -540,11 +604,11 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                     }
                     constexpr int kMove = (Smem::kStackCap - kSpillCount + 31) / 32;
                     const int rest = top - kSpillCount;  // <= kStackCap - kSpillCount
-                    int2 mv[kMove];
+                    Entry mv[kMove];
 #pragma unroll
                     for (int i = 0; i < kMove; ++i) {
                         const int j = lane + 32 * i;
-                        mv[i] = j < rest ? W.stk[kSpillCount + j] : make_int2(0, 0);
+                        mv[i] = j < rest ? W.stk[kSpillCount + j] : Entry{};
                     }
                     __syncwarp();
 #pragma unroll
@@ -553,17 +617,25 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                         if (j < rest) W.stk[j] = mv[i];
                     }
                     top = rest;
-                    if (kCount) A.spills += 1u;
+                    if (kCount) WC.spills += 1u;
                     __syncwarp();
                 }
             }
         }
-        if (nsrc > 0) flush_sources<H, kPot, kCount>(W, nsrc, lane, lane_bit, pos, G, p, eps2, leaf_thr, A);
-        if (valid)
-            acc[t] = make_float4(__fadd_rn(A.ax.x, A.ax.y), __fadd_rn(A.ay.x, A.ay.y), __fadd_rn(A.az.x, A.az.y),
-                                 __fadd_rn(A.pot.x, A.pot.y));
+        if (nsrc > 0) flush_sources<H, T, kPot, kCount>(W, nsrc, lane, lane_bit, pos, G, X, e2, leaf_thr, A, WC);
+#pragma unroll
+        for (int t = 0; t < T; ++t)
+            if (valid[t])
+                acc[grp.start + lane + 32 * t] =
+                    make_float4(__fadd_rn(A[t].ax.x, A[t].ax.y), __fadd_rn(A[t].ay.x, A[t].ay.y),
+                                __fadd_rn(A[t].az.x, A[t].az.y), __fadd_rn(A[t].pot.x, A[t].pot.y));
         if (kCount) {
-            unsigned long long cm = A.n_mono, cp = A.n_part;
+            unsigned long long cm = 0ull, cp = 0ull;
+#pragma unroll
+            for (int t = 0; t < T; ++t) {
+                cm += A[t].n_mono;
+                cp += A[t].n_part;
+            }
             for (int o = 16; o > 0; o >>= 1) {
                 cm += __shfl_xor_sync(kFull, cm, o);
                 cp += __shfl_xor_sync(kFull, cp, o);
@@ -571,12 +643,12 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
             if (lane == 0) {
                 atomicAdd(counts, cm);
                 atomicAdd(counts + 1, cp);
-                atomicAdd(counts + 2, (unsigned long long)A.w_node);
-                atomicAdd(counts + 3, (unsigned long long)A.w_src);
-                atomicAdd(counts + 4, (unsigned long long)A.rounds);
-                atomicAdd(counts + 5, (unsigned long long)A.spills);
-                atomicAdd(counts + 6, (unsigned long long)A.all_open);
-                atomicAdd(counts + 7, (unsigned long long)A.all_take);
+                atomicAdd(counts + 2, (unsigned long long)WC.w_node);
+                atomicAdd(counts + 3, (unsigned long long)WC.w_src);
+                atomicAdd(counts + 4, (unsigned long long)WC.rounds);
+                atomicAdd(counts + 5, (unsigned long long)WC.spills);
+                atomicAdd(counts + 6, (unsigned long long)WC.all_open);
+                atomicAdd(counts + 7, (unsigned long long)WC.all_take);
             }
         }
         __syncwarp();
@@ -594,47 +666,55 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
     }
 }
 
-template <int H>
+template <int H, int T>
 constexpr size_t smem_bytes() {
-    return sizeof(WarpSmem<H>) * kWalkWarps;
+    return sizeof(WarpSmem<H, T>) * kWalkWarps;
 }
 
-// Opt the instantiation in to its dynamic shared memory (above 48 KB for H=2).
-template <int H, bool kPot, bool kCount>
+// Opt the instantiation in to its dynamic shared memory (above 48 KB).
+template <int H, int T, bool kPot, bool kCount>
 void configure() {
     static bool done = false;
     if (!done) {
-        cudaFuncSetAttribute(walk_kernel<H, kPot, kCount>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem_bytes<H>());
+        cudaFuncSetAttribute(walk_kernel<H, T, kPot, kCount>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem_bytes<H, T>());
         done = true;
     }
 }
 
-template <int H, bool kPot, bool kCount>
+template <int H, int T, bool kPot, bool kCount>
 int occupancy_of() {
-    configure<H, kPot, kCount>();
+    configure<H, T, kPot, kCount>();
     int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, walk_kernel<H, kPot, kCount>, kWalkThreads,
-                                                  smem_bytes<H>());
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, walk_kernel<H, T, kPot, kCount>, kWalkThreads,
+                                                  smem_bytes<H, T>());
     return nb > 0 ? nb : 1;
 }
 
-}  // namespace
-
-int walk_max_blocks_per_sm(int batch, int with_potential) {
+template <int T>
+int max_blocks_of(int batch, int with_potential) {
     // the same for every device of this build (sm_100a only)
     static int cached[2][2] = {{0, 0}, {0, 0}};
     const int hi = batch > 32 ? 1 : 0, pot = with_potential ? 1 : 0;
     int& nb = cached[hi][pot];
     if (nb == 0) {
-        if (hi) nb = pot ? occupancy_of<2, true, false>() : occupancy_of<2, false, false>();
-        else nb = pot ? occupancy_of<1, true, false>() : occupancy_of<1, false, false>();
+        if (hi) nb = pot ? occupancy_of<2, T, true, false>() : occupancy_of<2, T, false, false>();
+        else nb = pot ? occupancy_of<1, T, true, false>() : occupancy_of<1, T, false, false>();
     }
     return nb;
 }
 
+}  // namespace
+
+int walk_max_blocks_per_sm(int batch, int with_potential, int targets_per_lane) {
+    return targets_per_lane > 1 ? max_blocks_of<2>(batch, with_potential) : max_blocks_of<1>(batch, with_potential);
+}
+
 int64_t walk_grid_blocks(int n_groups, int blocks_per_sm, int sm_count, int with_potential) {
-    const int max_b = std::max(walk_max_blocks_per_sm(32, with_potential), walk_max_blocks_per_sm(64, with_potential));
+    int max_b = 0;
+    for (int t = 1; t <= 2; ++t)
+        max_b = std::max(max_b, std::max(walk_max_blocks_per_sm(32, with_potential, t),
+                                         walk_max_blocks_per_sm(64, with_potential, t)));
     const int bps = blocks_per_sm > 0 && blocks_per_sm < max_b ? blocks_per_sm : max_b;
     int64_t grid = (int64_t)sm_count * bps;
     const int64_t need = ((int64_t)n_groups + kWalkWarps - 1) / kWalkWarps;
@@ -646,35 +726,36 @@ size_t walk_stack_entries(int64_t grid_blocks) {
     return (size_t)grid_blocks * kWalkWarps * (size_t)kWalkGlobalStack;
 }
 
-template <int H>
-static void launch_h(const Layout& L, const WalkParams& q, const float4* pos, const WalkNode* tr,
-                     const WalkGroup* groups, int n_groups, float4* acc, uint32_t* queue, uint32_t* status,
-                     unsigned long long* counts, int2* gstack, unsigned g, cudaStream_t st) {
-    const int cap = kWalkGlobalStack;
-    const size_t sm = smem_bytes<H>();
+template <int H, int T>
+static void launch_ht(const Layout& L, const WalkParams& q, const float4* pos, const WalkNode* wn,
+                      const WalkGroup* groups, int n_groups, float4* acc, uint32_t* queue, uint32_t* status,
+                      unsigned long long* counts, int2* gstack, int cap, unsigned g, cudaStream_t st) {
+    using Entry = typename EntryOf<T>::type;
+    Entry* gs = reinterpret_cast<Entry*>(gstack);
+    const size_t sm = smem_bytes<H, T>();
     if (counts) {
         if (q.with_potential) {
-            configure<H, true, true>();
-            walk_kernel<H, true, true><<<g, kWalkThreads, sm, st>>>(L, q, pos, tr, groups, n_groups, acc, queue,
-                                                                    status, counts, gstack, cap);
+            configure<H, T, true, true>();
+            walk_kernel<H, T, true, true><<<g, kWalkThreads, sm, st>>>(L, q, pos, wn, groups, n_groups, acc, queue,
+                                                                       status, counts, gs, cap);
         } else {
-            configure<H, false, true>();
-            walk_kernel<H, false, true><<<g, kWalkThreads, sm, st>>>(L, q, pos, tr, groups, n_groups, acc,
-                                                                     queue, status, counts, gstack, cap);
+            configure<H, T, false, true>();
+            walk_kernel<H, T, false, true><<<g, kWalkThreads, sm, st>>>(L, q, pos, wn, groups, n_groups, acc, queue,
+                                                                        status, counts, gs, cap);
         }
     } else if (q.with_potential) {
-        configure<H, true, false>();
-        walk_kernel<H, true, false><<<g, kWalkThreads, sm, st>>>(L, q, pos, tr, groups, n_groups, acc, queue,
-                                                                 status, nullptr, gstack, cap);
+        configure<H, T, true, false>();
+        walk_kernel<H, T, true, false><<<g, kWalkThreads, sm, st>>>(L, q, pos, wn, groups, n_groups, acc, queue,
+                                                                    status, nullptr, gs, cap);
     } else {
-        configure<H, false, false>();
-        walk_kernel<H, false, false><<<g, kWalkThreads, sm, st>>>(L, q, pos, tr, groups, n_groups, acc, queue,
-                                                                  status, nullptr, gstack, cap);
+        configure<H, T, false, false>();
+        walk_kernel<H, T, false, false><<<g, kWalkThreads, sm, st>>>(L, q, pos, wn, groups, n_groups, acc, queue,
+                                                                     status, nullptr, gs, cap);
     }
 }
 
 void launch_walk(const Layout& L, const WalkParams& wp, const float4* pos,
-                 const WalkNode* tr, const WalkGroup* groups, int n_groups, float4* acc,
+                 const WalkNode* wn, const WalkGroup* groups, int n_groups, int targets_per_lane, float4* acc,
                  uint32_t* queue, uint32_t* status, int blocks_per_sm, int sm_count,
                  unsigned long long* counts, int2* gstack, size_t gstack_entries, cudaStream_t st) {
     if (n_groups <= 0) return;
@@ -683,20 +764,32 @@ void launch_walk(const Layout& L, const WalkParams& wp, const float4* pos,
     if (q.batch > kWalkMaxBatch) q.batch = kWalkMaxBatch;
     if (q.leaf_size < 1) q.leaf_size = 1;
     if (q.leaf_size > 32) q.leaf_size = 32;
-    const int max_b = walk_max_blocks_per_sm(q.batch, q.with_potential);
+    const int T = targets_per_lane > 1 ? 2 : 1;
+    const int max_b = walk_max_blocks_per_sm(q.batch, q.with_potential, T);
     const int bps = blocks_per_sm > 0 && blocks_per_sm < max_b ? blocks_per_sm : max_b;
     int64_t grid = (int64_t)sm_count * bps;
     const int64_t need = ((int64_t)n_groups + kWalkWarps - 1) / kWalkWarps;
     if (grid > need) grid = need;
-    // never more warps than the global stack regions provided
+    // never more warps than the global stack regions provided: the int2
+    // buffer holds kWalkGlobalStack 8-byte units per warp; a T = 2 entry
+    // takes two of them
     const int64_t fit = (int64_t)(gstack_entries / ((size_t)kWalkWarps * kWalkGlobalStack));
     if (grid > fit) grid = fit;
     if (grid < 1) return;  // no stack regions: nothing can run (the engine always provides them)
     const unsigned g = (unsigned)grid;
-    if (q.batch > 32)
-        launch_h<2>(L, q, pos, tr, groups, n_groups, acc, queue, status, counts, gstack, g, st);
-    else
-        launch_h<1>(L, q, pos, tr, groups, n_groups, acc, queue, status, counts, gstack, g, st);
+    // entries per warp region: the whole buffer split over this grid's warps
+    const size_t units = gstack_entries / ((size_t)grid * kWalkWarps);
+    const int cap = (int)(std::min<size_t>(units, (size_t)1 << 24) / (size_t)T);
+    if (T == 2) {
+        if (q.batch > 32)
+            launch_ht<2, 2>(L, q, pos, wn, groups, n_groups, acc, queue, status, counts, gstack, cap, g, st);
+        else
+            launch_ht<1, 2>(L, q, pos, wn, groups, n_groups, acc, queue, status, counts, gstack, cap, g, st);
+    } else if (q.batch > 32) {
+        launch_ht<2, 1>(L, q, pos, wn, groups, n_groups, acc, queue, status, counts, gstack, cap, g, st);
+    } else {
+        launch_ht<1, 1>(L, q, pos, wn, groups, n_groups, acc, queue, status, counts, gstack, cap, g, st);
+    }
 }
 
 }  // namespace gcs

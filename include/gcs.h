@@ -111,9 +111,10 @@ int64_t gcs_segment_offset(const gcs_ctx* ctx, int32_t segment);
 int64_t gcs_num_particles(const gcs_ctx* ctx);
 int32_t gcs_num_segments(const gcs_ctx* ctx);
 
-/* Targets per walk group (8..32, default 32): the walk's warps each take a
- * run of this many consecutive sorted particles of one segment.  Results do
- * not depend on it (each target's terms are its own walk's); speed does. */
+/* Targets per walk group (8..64, default 32): the walk's warps each take a
+ * run of this many consecutive sorted particles of one segment (above 32, two
+ * targets per lane).  Results do not depend on it (each target's terms are
+ * its own walk's); speed does. */
 int gcs_set_group_width(gcs_ctx* ctx, int32_t width);
 int32_t gcs_group_width(const gcs_ctx* ctx);
 

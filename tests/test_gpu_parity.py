@@ -171,6 +171,50 @@ def test_walk_batch_sizes_agree(gcs_mod, stars, batch):
         _assert_acc(a2[:, :3], a1[:, :3])
 
 
+@pytest.mark.parametrize("width,batch,theta,leaf", [(64, 64, 0.5, 4), (64, 32, 0.5, 1), (64, 64, 1.0, 1),
+                                                   (48, 64, 0.7, 8), (40, 16, 0.5, 32)])
+def test_wide_groups_match_oracle(gcs_mod, oracle_mod, stars, width, batch, theta, leaf):
+    """Groups wider than 32 hold two targets per lane; every target still
+    takes exactly its own terms: accelerations within the walk tolerance of
+    the oracle and the same number of monopole and particle terms as the
+    oracle's per-target walk."""
+    gcs = gcs_mod
+    with _ctx(gcs, stars) as ctx:
+        ctx.set_group_width(width)
+        assert ctx.group_width == width
+        p = _params(gcs, theta=theta, leaf_size=leaf, walk_batch=batch, with_potential=1)
+        ctx.run_stages(p, gcs.STAGE_BOUNDS, gcs.STAGE_WALK)
+        sp = ctx.read(gcs.BUF_POS)
+        nodes = ctx.read(gcs.BUF_NODES)
+        acc = ctx.read(gcs.BUF_ACCEL)
+        ref, cnt = oracle_mod.walk(sp, nodes, p.G, p.epsilon_sq, theta, leaf, counts=True)
+        _assert_acc(acc[:, :3], ref[:, :3], "width=%d batch=%d theta=%s L=%d" % (width, batch, theta, leaf))
+        np.testing.assert_allclose(acc[:, 3], ref[:, 3], rtol=1e-5)
+        n_mono, n_part = ctx.count_interactions(p)
+        assert (n_mono, n_part) == (int(cnt[:, 0].sum()), int(cnt[:, 1].sum()))
+        assert ctx.device_status() == 0
+
+
+def test_wide_groups_in_segments(gcs_mod, stars):
+    """Two targets per lane over uneven segments (groups never straddle a
+    segment): each segment's accelerations equal the segment walked alone."""
+    gcs = gcs_mod
+    a = small_collision(700, 170, 91, seed=21)   # 1,922 particles: not a multiple of 64
+    b = small_collision(300, 64, 33, seed=22)    # 794
+    p = _params(gcs, leaf_size=4, walk_batch=64)
+    with _ctx(gcs, np.concatenate([a, b]), segments=[len(a), len(b)]) as both:
+        both.set_group_width(64)
+        both.run_stages(p, gcs.STAGE_BOUNDS, gcs.STAGE_WALK)
+        acc_both = both.read(gcs.BUF_ACCEL)
+        assert both.device_status() == 0
+    for k, part in enumerate((a, b)):
+        with _ctx(gcs, part) as solo:
+            solo.set_group_width(64)
+            solo.run_stages(p, gcs.STAGE_BOUNDS, gcs.STAGE_WALK)
+            off = 0 if k == 0 else len(a)
+            assert np.array_equal(solo.read(gcs.BUF_ACCEL), acc_both[off:off + len(part)])
+
+
 def test_group_width_and_autotune(gcs_mod, oracle_mod, stars):
     """Group width changes only the order of the sums; the autotuner returns
     settings within the caller's leaf bound whose results match the oracle."""
