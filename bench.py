@@ -423,17 +423,28 @@ def batched_bench(gcs, torch, args):
     seq_s = 0.0
     with gcs.Context(max(counts)) as ctx:
         ctx.set_stream(stream.cuda_stream)
-        ctx.set_group_width(width)
+        # the one-at-a-time path gets its own tuning: the autotuner on three
+        # representative sizes (quartile, median, 90th percentile); each
+        # scenario runs with the settings of the nearest size (log scale)
+        order = np.argsort(counts)
+        reps = sorted({int(order[int(q * (len(order) - 1))]) for q in (0.25, 0.5, 0.9)})
+        tuned = []
+        for r in reps:
+            ctx.set_segments([counts[r]])
+            ctx.upload(stars[r])
+            tuned.append((counts[r], _tune(gcs, ctx), ctx.group_width))
         ctx.set_graphs(True)
         for st in stars:
+            _, q, w = min(tuned, key=lambda t: abs(np.log(t[0] / len(st))))
+            ctx.set_group_width(w)
             ctx.set_segments([len(st)])
             ctx.upload(st)
             for _ in range(W):
-                ctx.step(p)
+                ctx.step(q)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
             for _ in range(K):
-                ctx.step(p)
+                ctx.step(q)
             e1.record(stream)
             e1.synchronize()
             seq_s += e0.elapsed_time(e1) / 1e3
@@ -448,7 +459,10 @@ def batched_bench(gcs, torch, args):
             "batched": {"value": rb, "unit": "particle-steps/s", "ms_per_step": t_batched * 1e3 / K,
                         "graph_builds": builds},
             "one_at_a_time": {"value": rs, "unit": "particle-steps/s", "seconds": seq_s,
-                              "path": "one segment per context layout, graph-captured step, same parameters"},
+                              "path": "one segment per context layout, graph-captured step, autotuned on "
+                                      "three representative sizes",
+                              "tuned": [{"particles": c, "leaf_size": q.leaf_size, "walk_batch": q.walk_batch,
+                                         "group_width": w} for c, q, w in tuned]},
             "speedup": rb / rs, "leaf_size": p.leaf_size, "walk_batch": p.walk_batch, "group_width": width,
             "ic_seconds": gen_s}
 

@@ -94,7 +94,7 @@ struct gcs_ctx {
 
 namespace {
 
-constexpr int kChunkSize = 8192;
+constexpr int kChunkSize = 2048;  // particles per bounds block
 constexpr int kCountWords = 8;  // counting-walk outputs (gcs_count_interactions)
 constexpr int kMinGroupWidth = 8;
 

@@ -89,16 +89,27 @@ __global__ void pack_playback_kernel(const float4* __restrict__ pos, const float
 __global__ void bounds_kernel(const float4* __restrict__ pos, const Chunk* __restrict__ chunks,
                               int n_chunks, uint32_t* __restrict__ bounds_enc,
                               uint32_t* __restrict__ status) {
+    constexpr int kInFlight = 8;  // independent loads per thread per sweep
     __shared__ float s_lo[kStreamThreads / 32], s_hi[kStreamThreads / 32];
     for (int c = blockIdx.x; c < n_chunks; c += gridDim.x) {
         const Chunk ch = chunks[c];
         float lo = INFINITY, hi = -INFINITY;
         bool bad = false;
-        for (int i = threadIdx.x; i < ch.count; i += blockDim.x) {
-            const float4 p = __ldg(pos + ch.start + i);
-            bad |= !(isfinite(p.x) && isfinite(p.y) && isfinite(p.z));
-            lo = fminf(lo, fminf(p.x, fminf(p.y, p.z)));
-            hi = fmaxf(hi, fmaxf(p.x, fmaxf(p.y, p.z)));
+        for (int i0 = threadIdx.x; i0 < ch.count; i0 += kInFlight * blockDim.x) {
+            float4 p[kInFlight];
+#pragma unroll
+            for (int k = 0; k < kInFlight; ++k) {
+                const int i = i0 + k * blockDim.x;
+                p[k] = i < ch.count ? __ldg(pos + ch.start + i) : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+#pragma unroll
+            for (int k = 0; k < kInFlight; ++k) {
+                if (i0 + k * (int)blockDim.x < ch.count) {
+                    bad |= !(isfinite(p[k].x) && isfinite(p[k].y) && isfinite(p[k].z));
+                    lo = fminf(lo, fminf(p[k].x, fminf(p[k].y, p[k].z)));
+                    hi = fmaxf(hi, fmaxf(p[k].x, fmaxf(p[k].y, p[k].z)));
+                }
+            }
         }
         if (__any_sync(0xFFFFFFFFu, bad) && (threadIdx.x & 31) == 0)
             atomicOr(status, GCS_DEV_NONFINITE_POSITION);
