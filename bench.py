@@ -208,6 +208,22 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi, 200 ms"}
 
 
+def replica_throughput(n_local, steps, t_local_s, dist=None, device="cpu"):
+    """Whole-job particle-steps/s of independent replicas (one scenario per
+    rank, no data-path collective): the particles of every rank over the
+    slowest rank's time.  Returns (value, max time over ranks in s, particles
+    over ranks).  Every rank must call it (two all-reduces)."""
+    if dist is None:
+        return n_local * steps / t_local_s, t_local_s, n_local
+    import torch  # noqa: PLC0415
+    t = torch.tensor([float(t_local_s)], dtype=torch.float64, device=device)
+    n = torch.tensor([float(n_local)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(n, op=dist.ReduceOp.SUM)
+    t_max, n_all = float(t.item()), int(n.item())
+    return n_all * steps / t_max, t_max, n_all
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -652,12 +668,8 @@ def main():
         raise RuntimeError("device status word 0x%x after the timed steps" % status)
     t_ms = ev0.elapsed_time(ev1)
     walk_ms = sum(a.elapsed_time(b) for a, b in wev) / args.steps
-    t_max = t_ms
-    if dist is not None:
-        tt = torch.tensor([t_ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt.item())
-    value = n * args.steps * world / (t_max / 1e3)
+    value, t_max_s, _ = replica_throughput(n, args.steps, t_ms / 1e3, dist, "cuda")
+    t_max = t_max_s * 1e3
 
     # ---- end to end through the C ABI with host buffers
     host = torch.empty(n * 32, dtype=torch.uint8, pin_memory=True)
@@ -671,11 +683,8 @@ def main():
         ctx.upload(hv)
         ctx.step_host(p, hv)
     t_e2e = time.perf_counter() - t0
-    if dist is not None:
-        tt = torch.tensor([t_e2e], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_e2e = float(tt.item())
-    e2e = {"value": n * ke * world / t_e2e, "unit": "particle-steps/s", "h2d_bytes_per_step": 32 * n,
+    e2e_value, t_e2e, _ = replica_throughput(n, ke, t_e2e, dist, "cuda")
+    e2e = {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": 32 * n,
            "d2h_bytes_per_step": 32 * n, "steps": ke,
            "path": "gcs_upload_stars (pinned Star[] H2D) + gcs_step_host (step, pack, Star[] D2H)"}
 
