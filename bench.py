@@ -65,6 +65,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-render", action="store_true")
+    ap.add_argument("--no-bake", action="store_true")
     ap.add_argument("--batched-count", type=int, default=256)
     ap.add_argument("--batched-steps", type=int, default=10)
     ap.add_argument("--no-served", action="store_true")
@@ -400,6 +401,40 @@ def render_bench(gcs, torch, ctx, stream, frames=10, width=1920, height=1080):
     return res
 
 
+def bake_bench(gcs, ctx, p, frames=10):
+    """simulation.bin baking of the benchmark state: the pipelined gcs_bake
+    (device packing, copies on a second stream, writer thread) against the
+    reference Bake loop's shape run through the same engine (step, read the
+    frame back, write it, one after another).  Files go to the temporary
+    directory and are removed."""
+    import tempfile  # noqa: PLC0415
+    n = ctx.n
+    out = {"workload": "%d frames of %d particles (%.1f MB per frame)" % (frames, n, 16 * n / 1e6)}
+    d = tempfile.mkdtemp(prefix="gcs_bake_")
+    try:
+        path = os.path.join(d, "simulation.bin")
+        ctx.bake(p, 1, path)  # warm-up: pinned buffers, first write
+        sec = ctx.bake(p, frames, path)
+        out["pipelined"] = {"frames_per_s": frames / sec, "particle_steps_per_s": n * frames / sec, "seconds": sec}
+        path2 = os.path.join(d, "serial.bin")
+        t0 = time.perf_counter()
+        with open(path2, "wb") as f:
+            for _ in range(frames):
+                ctx.step(p)
+                f.write(ctx.download_playback().tobytes())
+        sec2 = time.perf_counter() - t0
+        out["step_then_write"] = {"frames_per_s": frames / sec2, "particle_steps_per_s": n * frames / sec2,
+                                  "seconds": sec2}
+    finally:
+        for name in ("simulation.bin", "serial.bin"):
+            try:
+                os.remove(os.path.join(d, name))
+            except OSError:
+                pass
+        os.rmdir(d)
+    return out
+
+
 def batched_bench(gcs, torch, args):
     """256 uneven scenarios: all advanced together (segments of one context,
     one launch per stage, graph-captured step) versus the same scenarios one
@@ -722,6 +757,8 @@ def main():
             line["cpu_baseline"] = cpu_reference_rate(stars, args.cpu_seconds)
         if not args.no_render:
             line["render"] = render_bench(gcs, torch, ctx, stream)
+        if not args.no_bake:
+            line["bake"] = bake_bench(gcs, ctx, p)
     ctx.close()
     if rank == 0 and world == 1:
         if not args.no_batched:

@@ -7,10 +7,14 @@
 // device), all work is asynchronous on the context's stream with no device
 // synchronisation between stages, and every failure is a status code.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "gcs_internal.h"
@@ -1084,3 +1088,134 @@ int gcs_render_stars(const Star* stars, int64_t n, const gcs_camera* cam, int32_
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// bake: steps written as simulation.bin frames (main.cpp:119-297)
+// ---------------------------------------------------------------------------
+// The reference's Bake loop steps synchronously, copies the Star array to
+// the host, converts it to PlaybackStar records on the host and hands the
+// frame to a writer thread.  Here each frame is packed on the device
+// (launch_pack_playback, the same records gcs_download_playback returns),
+// copied on a second stream into one of two pinned buffers while the next
+// step computes, and written by a writer thread in frame order.
+namespace {
+
+struct BakeWriter {
+    std::mutex mu;
+    std::condition_variable cv;
+    int64_t queued = 0;   // frames handed to the writer
+    int64_t written = 0;  // frames written (or abandoned after an error)
+    bool stop = false;
+    int error = 0;
+};
+
+}  // namespace
+
+extern "C" int gcs_bake(gcs_ctx* c, const gcs_params* p, int32_t frames, const char* path, int32_t append,
+                        double* seconds) {
+    if (!c || !p || !path || frames < 0) return GCS_ERR_ARG;
+    int rc = validate_params(c, p);
+    if (rc) return rc;
+    const auto t0 = std::chrono::steady_clock::now();
+    FILE* f = std::fopen(path, append ? "ab" : "wb");
+    if (!f) {
+        c->last_error = std::string("bake: cannot open ") + path;
+        return GCS_ERR_ARG;
+    }
+    cudaSetDevice(c->device);
+    const int64_t n = c->n;
+    const size_t bytes = sizeof(PlaybackStar) * (size_t)n;
+    PlaybackStar* host[2] = {nullptr, nullptr};
+    cudaStream_t copy = nullptr;
+    cudaEvent_t packed[2] = {nullptr, nullptr}, copied[2] = {nullptr, nullptr};
+    bool ok = cudaMallocHost(reinterpret_cast<void**>(&host[0]), bytes > 0 ? bytes : 1) == cudaSuccess &&
+              cudaMallocHost(reinterpret_cast<void**>(&host[1]), bytes > 0 ? bytes : 1) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&copy, cudaStreamNonBlocking) == cudaSuccess;
+    for (int b = 0; b < 2 && ok; ++b)
+        ok = cudaEventCreateWithFlags(&packed[b], cudaEventDisableTiming) == cudaSuccess &&
+             cudaEventCreateWithFlags(&copied[b], cudaEventDisableTiming) == cudaSuccess;
+    BakeWriter W;
+    std::thread writer;
+    if (ok) {
+        writer = std::thread([&]() {
+            for (int64_t k = 0;; ++k) {
+                {
+                    std::unique_lock<std::mutex> lk(W.mu);
+                    W.cv.wait(lk, [&] { return W.queued > k || W.stop; });
+                    if (W.queued <= k) return;
+                }
+                int err = 0;
+                if (cudaEventSynchronize(copied[k & 1]) != cudaSuccess) err = GCS_ERR_CUDA;
+                else if (n > 0 && std::fwrite(host[k & 1], sizeof(PlaybackStar), (size_t)n, f) != (size_t)n)
+                    err = GCS_ERR_ARG;
+                {
+                    std::lock_guard<std::mutex> lk(W.mu);
+                    if (err && !W.error) W.error = err;
+                    W.written = k + 1;
+                }
+                W.cv.notify_all();
+            }
+        });
+    } else {
+        c->last_error = "bake: pinned buffers, copy stream or events could not be created";
+        rc = GCS_ERR_NOMEM;
+    }
+    for (int32_t k = 0; ok && k < frames; ++k) {
+        if ((rc = gcs_step(c, p))) break;
+        // the staging buffer is free again once the previous frame's copy is done
+        if (k >= 1 && cudaStreamWaitEvent(c->stream, copied[(k - 1) & 1], 0) != cudaSuccess) {
+            rc = GCS_ERR_CUDA;
+            break;
+        }
+        if (n > 0) launch_pack_playback(c->pos[c->cur], c->vel[c->cur], c->pb_staging, n, c->stream);
+        if ((rc = check_launch(c, "bake pack")) || cudaEventRecord(packed[k & 1], c->stream) != cudaSuccess) {
+            rc = rc ? rc : GCS_ERR_CUDA;
+            break;
+        }
+        {
+            // host buffer k & 1 is free once frame k - 2 has been written
+            std::unique_lock<std::mutex> lk(W.mu);
+            W.cv.wait(lk, [&] { return W.written >= (int64_t)k - 1 || W.error; });
+            if (W.error) break;
+        }
+        if (cudaStreamWaitEvent(copy, packed[k & 1], 0) != cudaSuccess ||
+            (n > 0 && cudaMemcpyAsync(host[k & 1], c->pb_staging, bytes, cudaMemcpyDeviceToHost, copy) != cudaSuccess) ||
+            cudaEventRecord(copied[k & 1], copy) != cudaSuccess) {
+            rc = GCS_ERR_CUDA;
+            break;
+        }
+        {
+            std::lock_guard<std::mutex> lk(W.mu);
+            W.queued = (int64_t)k + 1;
+        }
+        W.cv.notify_all();
+    }
+    if (writer.joinable()) {
+        {
+            std::lock_guard<std::mutex> lk(W.mu);
+            W.stop = true;
+        }
+        W.cv.notify_all();
+        writer.join();
+    }
+    if (!rc && W.error) {
+        rc = W.error;
+        c->last_error = rc == GCS_ERR_CUDA ? "bake: frame copy failed" : "bake: short write of a frame";
+    }
+    if (std::fclose(f) != 0 && !rc) {
+        rc = GCS_ERR_ARG;
+        c->last_error = "bake: closing the output failed";
+    }
+    if (copy) {
+        cudaStreamSynchronize(copy);
+        cudaStreamDestroy(copy);
+    }
+    for (int b = 0; b < 2; ++b) {
+        if (packed[b]) cudaEventDestroy(packed[b]);
+        if (copied[b]) cudaEventDestroy(copied[b]);
+        if (host[b]) cudaFreeHost(host[b]);
+    }
+    if (!rc) rc = gcs_synchronize(c);
+    if (seconds) *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return rc;
+}

@@ -131,6 +131,7 @@ def lib() -> C.CDLL:
         "gcs_segment_offset": (i64, [P, i32]),
         "gcs_device_bytes": (i64, [P]),
         "gcs_context_bytes": (i64, [i64, i32, i32]),
+        "gcs_bake": (C.c_int, [P, C.POINTER(Params), i32, C.c_char_p, i32, C.POINTER(C.c_double)]),
         "gcs_camera_reference": (None, [C.POINTER(Camera)]),
         "gcs_camera_matrices": (C.c_int, [C.POINTER(Camera), i32, i32, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
         "gcs_render_frame": (C.c_int, [P, C.POINTER(Camera), i32, i32, i32, P, i32]),
@@ -362,6 +363,13 @@ class Context:
         self.check(self.L.gcs_count_interactions(self._h, C.byref(p), out))
         r = tuple(int(x) for x in out)
         return r if warp_evals else r[:2]
+
+    def bake(self, p: Params, frames: int, path: str, append: bool = False) -> float:
+        """`frames` steps, each written as a simulation.bin frame to `path`;
+        returns the wall time in seconds."""
+        sec = C.c_double(0.0)
+        self.check(self.L.gcs_bake(self._h, C.byref(p), frames, path.encode(), int(append), C.byref(sec)))
+        return sec.value
 
     def render(self, cam: "Camera", width: int, height: int, segment: int = -1) -> np.ndarray:
         """The headless splat frame of the current particles: (height, width, 4)

@@ -292,6 +292,18 @@ int64_t gcs_device_bytes(const gcs_ctx* ctx);
  * (nothing is allocated); a negative status on bad arguments or device. */
 int64_t gcs_context_bytes(int64_t capacity, int32_t max_segments, int32_t device);
 
+/* ---- bake --------------------------------------------------------------------
+ * `frames` steps of every segment, each followed by one simulation.bin frame
+ * (n PlaybackStar records of the stepped state in that step's order, the
+ * records gcs_download_playback returns) appended to `path` (created, or
+ * appended to with append = 1): the reference's Bake loop (main.cpp:119-297).
+ * Frames are packed on the device, copied into two pinned buffers on a
+ * second stream while the next step computes, and written by a writer
+ * thread in order.  Returns when every frame is on disk; seconds (may be
+ * NULL) receives the wall time. */
+int gcs_bake(gcs_ctx* ctx, const gcs_params* p, int32_t frames, const char* path, int32_t append,
+             double* seconds);
+
 /* ---- headless point-splat renderer ------------------------------------------
  * The reference draws every Star as one GL point (renderer.cpp:97-148,
  * vertex attributes 226-233): the
