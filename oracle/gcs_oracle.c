@@ -236,61 +236,88 @@ static void add_term(float gm, float dx, float dy, float dz, float d2, float* a)
  * cuda_engine.cu:143) and leaf size L (an opened node of <= L particles is
  * summed directly).  Leaves use the 1.01 eps^2 exclusion
  * (cuda_engine.cu:134).  Depth-first, left pushed before right. */
-void gcs_oracle_walk(int n, const float* xyzm, const BvhNodeTraverse* nodes, float G, float eps2,
-                     float theta, int leaf_size, float* acc, int64_t* counts) {
+/* One target's walk (cuda_engine.cu:91-161 with theta and leaf size L):
+ * acc4 gets ax, ay, az, potential; nm / np the monopole and particle terms. */
+static void walk_one(int t, int n, const float* xyzm, const BvhNodeTraverse* nodes, float G, float eps2,
+                     float theta2, float leaf_thr, int leaf_size, float* acc4, int64_t* nm_out, int64_t* np_out) {
     const int ni = n - 1;
-    const float theta2 = theta * theta;
-    const float leaf_thr = eps2 * 1.01f;
     int stack[256];
-    for (int t = 0; t < n; ++t) {
-        const float px = xyzm[4 * t], py = xyzm[4 * t + 1], pz = xyzm[4 * t + 2];
-        float a[4] = {0.f, 0.f, 0.f, 0.f};
-        int64_t nm = 0, np = 0;
-        if (n >= 2) {
-            int top = 0;
-            stack[top++] = 0;
-            while (top > 0) {
-                const int c = stack[--top];
-                if (c >= ni) {
-                    const float* q = xyzm + 4 * (size_t)(c - ni);
-                    const float dx = q[0] - px, dy = q[1] - py, dz = q[2] - pz;
-                    const float d2 = softened_d2(dx, dy, dz, eps2);
-                    if (d2 > leaf_thr) {
-                        add_term(G * q[3], dx, dy, dz, d2, a);
+    const float px = xyzm[4 * (size_t)t], py = xyzm[4 * (size_t)t + 1], pz = xyzm[4 * (size_t)t + 2];
+    float a[4] = {0.f, 0.f, 0.f, 0.f};
+    int64_t nm = 0, np = 0;
+    if (n >= 2) {
+        int top = 0;
+        stack[top++] = 0;
+        while (top > 0) {
+            const int c = stack[--top];
+            if (c >= ni) {
+                const float* q = xyzm + 4 * (size_t)(c - ni);
+                const float dx = q[0] - px, dy = q[1] - py, dz = q[2] - pz;
+                const float d2 = softened_d2(dx, dy, dz, eps2);
+                if (d2 > leaf_thr) {
+                    add_term(G * q[3], dx, dy, dz, d2, a);
+                    ++np;
+                }
+                continue;
+            }
+            const BvhNodeTraverse* nd = nodes + c;
+            const float dx = nd->com_x - px, dy = nd->com_y - py, dz = nd->com_z - pz;
+            const float d2 = softened_d2(dx, dy, dz, eps2);
+            if (nd->width * nd->width < d2 * theta2) {
+                add_term(G * nd->mass, dx, dy, dz, d2, a);
+                ++nm;
+                continue;
+            }
+            const int own = c, re = nd->range_end;
+            const int lo = own < re ? own : re, hi = own < re ? re : own;
+            if (hi - lo + 1 <= leaf_size) {
+                for (int s = lo; s <= hi; ++s) {
+                    const float* q = xyzm + 4 * (size_t)s;
+                    const float ex = q[0] - px, ey = q[1] - py, ez = q[2] - pz;
+                    const float e2 = softened_d2(ex, ey, ez, eps2);
+                    if (e2 > leaf_thr) {
+                        add_term(G * q[3], ex, ey, ez, e2, a);
                         ++np;
                     }
-                    continue;
                 }
-                const BvhNodeTraverse* nd = nodes + c;
-                const float dx = nd->com_x - px, dy = nd->com_y - py, dz = nd->com_z - pz;
-                const float d2 = softened_d2(dx, dy, dz, eps2);
-                if (nd->width * nd->width < d2 * theta2) {
-                    add_term(G * nd->mass, dx, dy, dz, d2, a);
-                    ++nm;
-                    continue;
-                }
-                const int own = c, re = nd->range_end;
-                const int lo = own < re ? own : re, hi = own < re ? re : own;
-                if (hi - lo + 1 <= leaf_size) {
-                    for (int s = lo; s <= hi; ++s) {
-                        const float* q = xyzm + 4 * (size_t)s;
-                        const float ex = q[0] - px, ey = q[1] - py, ez = q[2] - pz;
-                        const float e2 = softened_d2(ex, ey, ez, eps2);
-                        if (e2 > leaf_thr) {
-                            add_term(G * q[3], ex, ey, ez, e2, a);
-                            ++np;
-                        }
-                    }
-                    continue;
-                }
-                stack[top++] = nd->child_left;
-                stack[top++] = nd->child_right;
+                continue;
             }
+            if (top + 2 > 256) break; /* deeper than any valid tree of < 2^31 particles */
+            stack[top++] = nd->child_left;
+            stack[top++] = nd->child_right;
         }
-        for (int k = 0; k < 4; ++k) acc[4 * (size_t)t + k] = a[k];
+    }
+    for (int k = 0; k < 4; ++k) acc4[k] = a[k];
+    *nm_out = nm;
+    *np_out = np;
+}
+
+void gcs_oracle_walk(int n, const float* xyzm, const BvhNodeTraverse* nodes, float G, float eps2,
+                     float theta, int leaf_size, float* acc, int64_t* counts) {
+    const float theta2 = theta * theta;
+    const float leaf_thr = eps2 * 1.01f;
+    for (int t = 0; t < n; ++t) {
+        int64_t nm, np;
+        walk_one(t, n, xyzm, nodes, G, eps2, theta2, leaf_thr, leaf_size, acc + 4 * (size_t)t, &nm, &np);
         if (counts) {
             counts[2 * (size_t)t] = nm;
             counts[2 * (size_t)t + 1] = np;
+        }
+    }
+}
+
+void gcs_oracle_walk_targets(int n, const float* xyzm, const BvhNodeTraverse* nodes, float G, float eps2,
+                             float theta, int leaf_size, const int64_t* targets, int64_t n_targets, float* acc,
+                             int64_t* counts) {
+    const float theta2 = theta * theta;
+    const float leaf_thr = eps2 * 1.01f;
+    for (int64_t k = 0; k < n_targets; ++k) {
+        int64_t nm, np;
+        walk_one((int)targets[k], n, xyzm, nodes, G, eps2, theta2, leaf_thr, leaf_size, acc + 4 * (size_t)k, &nm,
+                 &np);
+        if (counts) {
+            counts[2 * (size_t)k] = nm;
+            counts[2 * (size_t)k + 1] = np;
         }
     }
 }

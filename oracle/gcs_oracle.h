@@ -56,6 +56,11 @@ void gcs_oracle_aggregate(int n, const float* xyzm, BvhNodeTraverse* nodes, floa
  * 2 per particle (monopole terms, particle terms). */
 void gcs_oracle_walk(int n, const float* xyzm, const BvhNodeTraverse* nodes, float G, float eps2,
                      float theta, int leaf_size, float* acc, int64_t* counts);
+/* gcs_oracle_walk for the listed targets only (sorted indices): acc gets 4
+ * floats and counts (may be NULL) 2 per listed target. */
+void gcs_oracle_walk_targets(int n, const float* xyzm, const BvhNodeTraverse* nodes, float G, float eps2,
+                             float theta, int leaf_size, const int64_t* targets, int64_t n_targets, float* acc,
+                             int64_t* counts);
 /* cuda_engine.cu:164-216 (vel4: vx, vy, vz, bits of type|r|g|b). */
 void gcs_oracle_integrate(int64_t n, float* xyzm, float* vel4, const float* acc4, float dt,
                           int recolor);

@@ -47,6 +47,7 @@ def lib() -> C.CDLL:
             "gcs_oracle_walk": (None, [C.c_int, _P, _P, _f32, _f32, _f32, C.c_int, _P, _P]),
             "gcs_oracle_integrate": (None, [_i64, _P, _P, _P, _f32, C.c_int]),
             "gcs_oracle_render": (None, [_P, _i64, _P, _P, C.c_int, C.c_int, _P, _P]),
+            "gcs_oracle_walk_targets": (None, [C.c_int, _P, _P, _f32, _f32, _f32, C.c_int, _P, _i64, _P, _P]),
             "gcs_oracle_direct_fp64": (None, [_i64, _P, _P, _i64, _f64, _f64, _P]),
             "gcs_oracle_step": (None, [C.c_int, _P, _P, C.c_int, _f32, _f32, _f32, _f32, _f32, C.c_int,
                                        _f32, C.c_int, C.c_int, _P, _P]),
@@ -121,6 +122,21 @@ def walk(xyzm: np.ndarray, nodes: np.ndarray, G: float, eps2: float, theta: floa
     lib().gcs_oracle_walk(n, _ptr(x), _ptr(nd), G, eps2, theta, leaf_size, _ptr(acc),
                           _ptr(cnt) if counts else None)
     return (acc, cnt) if counts else acc
+
+
+def walk_targets(xyzm: np.ndarray, nodes: np.ndarray, G: float, eps2: float, theta: float, leaf_size: int,
+                 targets) -> tuple:
+    """walk() for the listed targets only -> (acc [k, 4], counts [k, 2])."""
+    x = f32(xyzm)
+    nd = np.ascontiguousarray(nodes, dtype=NODE_DTYPE)
+    if len(nd) == 0:
+        nd = np.zeros(1, NODE_DTYPE)
+    t = np.ascontiguousarray(targets, dtype=np.int64)
+    acc = np.zeros((len(t), 4), np.float32)
+    cnt = np.zeros((len(t), 2), np.int64)
+    lib().gcs_oracle_walk_targets(len(x), _ptr(x), _ptr(nd), G, eps2, theta, leaf_size, _ptr(t), len(t), _ptr(acc),
+                                  _ptr(cnt))
+    return acc, cnt
 
 
 def integrate(xyzm: np.ndarray, vel4: np.ndarray, acc4: np.ndarray, dt: float, recolor: bool = True):
