@@ -16,6 +16,8 @@
 //    histogram; keys of warp w precede those of warp w+1 and items are
 //    ranked in input order, so equal digits keep their input order (the sort
 //    is stable, which makes position the tie-break, karras_bvh.cuh:40);
+//  * a tile's keys and values are loaded right after its ticket, and the
+//    global digit starts are scanned while those loads are in flight;
 //  * look-back waits are bounded: a wait that runs out sets
 //    GCS_DEV_SORT_LOOKBACK_TIMEOUT, the tile still publishes (so later tiles
 //    finish) and skips its scatter, so nothing is written out of bounds;
@@ -69,7 +71,7 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* w
 }
 
 template <bool kSegPass>
-__global__ void __launch_bounds__(kSortThreads)
+__global__ void __launch_bounds__(kSortThreads, 2)
 onesweep_kernel(Layout L, int shift, const uint64_t* __restrict__ keys_in,
                 const uint32_t* __restrict__ vals_in, uint64_t* __restrict__ keys_out,
                 uint32_t* __restrict__ vals_out, const uint32_t* __restrict__ hist,
@@ -85,17 +87,18 @@ onesweep_kernel(Layout L, int shift, const uint64_t* __restrict__ keys_in,
         S.bad = 0;
     }
     for (int i = t; i < kWarps * kRadix; i += kSortThreads) (&S.whist[0][0])[i] = 0;
-    {
-        const uint32_t g = block_exclusive_scan(hist[t], S.warp_sums);  // t == digit
-        S.gbase[t] = g;
-    }
+    const uint32_t h = hist[t];  // t == digit
     __syncthreads();
     const uint32_t tile = S.tile;
     const int64_t tile_base = (int64_t)tile * kSortTile;
     const int64_t warp_base = tile_base + (int64_t)warp * (kSortItems * 32);
 
-    // ---- load and rank (warp-striped: item j of lane l is warp_base + 32j + l)
+    // ---- load (warp-striped: item j of lane l is warp_base + 32j + l); the
+    // values come with the keys and the global digit starts are scanned while
+    // the loads are in flight, so no later phase waits on global memory
+    // except the look-back
     uint64_t key[kSortItems];
+    uint32_t val[kSortItems];
     uint32_t rank[kSortItems];  // digit << 16 | rank within the warp's items
     const uint32_t lt_mask = (1u << lane) - 1u;
 #pragma unroll
@@ -103,9 +106,18 @@ onesweep_kernel(Layout L, int shift, const uint64_t* __restrict__ keys_in,
         const int64_t i = warp_base + 32 * j + lane;
         const bool valid = i < n;
         key[j] = valid ? keys_in[i] : 0ull;
+        val[j] = valid ? vals_in[i] : 0u;
+    }
+    S.gbase[t] = block_exclusive_scan(h, S.warp_sums);
+
+    // ---- rank
+#pragma unroll
+    for (int j = 0; j < kSortItems; ++j) {
+        const int64_t i = warp_base + 32 * j + lane;
+        const bool valid = i < n;
         uint32_t d;
         if (kSegPass) {
-            d = valid ? (((uint32_t)__ldg(L.seg_id + __ldg(vals_in + i)) >> shift) & (kRadix - 1)) : 0u;
+            d = valid ? (((uint32_t)__ldg(L.seg_id + val[j]) >> shift) & (kRadix - 1)) : 0u;
         } else {
             d = (uint32_t)(key[j] >> shift) & (kRadix - 1);
         }
@@ -188,7 +200,7 @@ onesweep_kernel(Layout L, int shift, const uint64_t* __restrict__ keys_in,
             const uint32_t d = rank[j] >> 16;
             const uint32_t lp = S.tstart[d] + S.whist[warp][d] + (rank[j] & 0xFFFFu);
             S.keys[lp] = key[j];
-            S.vals[lp] = vals_in[i];
+            S.vals[lp] = val[j];
             S.dig[lp] = (uint8_t)d;
         }
     }
