@@ -238,6 +238,17 @@ aggregate_kernel(Layout L, const float4* __restrict__ pos,
     int from = L.n_internal + g;
     ChildData mine = load_child(from, L.n_internal, pos, tr, bd, com64, fp64);
     int node = __ldg(leaf_parent + g);
+    // Links come from the build launch, so they can be read at any time: the
+    // first node's before the climb, each parent's as soon as the climb is
+    // known to continue to it (overlapping the sibling load and the node's
+    // arithmetic).
+    int cl = -1, cr = -1, up = -1, re = 0;
+    if (node >= 0 && node < L.n_internal) {
+        cl = __ldg(&tr[node].child_left);
+        cr = __ldg(&tr[node].child_right);
+        up = __ldg(&bd[node].parent);
+        re = __ldg(&tr[node].range_end);
+    }
     int levels = 0;
     while (node >= 0) {
         // a valid tree has at most 96 internal levels (strictly increasing
@@ -246,11 +257,6 @@ aggregate_kernel(Layout L, const float4* __restrict__ pos,
             atomicOr(status, GCS_DEV_TREE_MALFORMED);
             break;
         }
-        // links come from the build launch: fetch them before the arrival
-        const int cl = __ldg(&tr[node].child_left);
-        const int cr = __ldg(&tr[node].child_right);
-        const int up = __ldg(&bd[node].parent);
-        const int re = __ldg(&tr[node].range_end);
         const int own = node + s;  // particle index at this end of the node's range
         const bool local = min(own, re) >= b0 && max(own, re) < b0 + kAggThreads;
         int old;
@@ -278,6 +284,13 @@ aggregate_kernel(Layout L, const float4* __restrict__ pos,
             (cl != from && cr != from)) {
             atomicOr(status, GCS_DEV_TREE_MALFORMED);
             break;
+        }
+        int ncl = -1, ncr = -1, nup = -1, nre = 0;
+        if (up >= 0 && up < L.n_internal) {
+            ncl = __ldg(&tr[up].child_left);
+            ncr = __ldg(&tr[up].child_right);
+            nup = __ldg(&bd[up].parent);
+            nre = __ldg(&tr[up].range_end);
         }
         const bool left = cl == from;
         const int sib = left ? cr : cl;
@@ -347,6 +360,10 @@ aggregate_kernel(Layout L, const float4* __restrict__ pos,
         mine = next;
         from = node;
         node = up;
+        cl = ncl;
+        cr = ncr;
+        up = nup;
+        re = nre;
     }
 }
 
