@@ -240,7 +240,7 @@ __device__ __forceinline__ void flush_sources(WarpSmem<H, T>& W, int nsrc, int l
         for (int t = 0; t < T; ++t) put_mask(W.smask[t], e, m[t]);
     }
     __syncwarp();
-#pragma unroll 2
+#pragma unroll 4
     for (int q = 0; q < (padded >> 1); ++q) {
         const float4 zm = W.szm[q];
         const float4 xy = W.sxy[q];
@@ -468,7 +468,7 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                 }
                 // 3a. nodes every live target accepts: monopole terms, two
                 // nodes per packed evaluation, no masks
-#pragma unroll 2
+#pragma unroll 4
                 for (int q = 0; q < (take_base >> 1); ++q) {
                     const float4 zm = W.pzm[q];
                     const float4 xy = W.pxy[q];
@@ -484,7 +484,7 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                         if (valid[t]) A[t].n_mono += (uint32_t)n_full;
                 }
                 // 3b. nodes accepted by every target of their masks
-#pragma unroll 2
+#pragma unroll 4
                 for (int q = take_base >> 1; q < (mixed_base >> 1); ++q) {
                     const float4 zm = W.pzm[q];
                     const float4 xy = W.pxy[q];
@@ -499,6 +499,7 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                 }
                 // 3c. mixed nodes: each target's own test; lane 0 records the
                 // ballots of opening lanes for the nodes' owners
+#pragma unroll 2
                 for (int q = mixed_base >> 1; q < ((mixed_base + n_mixed + 1) >> 1); ++q) {
                     const float4 zm = W.pzm[q];
                     const float4 xy = W.pxy[q];
