@@ -401,7 +401,7 @@ def render_bench(gcs, torch, ctx, stream, frames=10, width=1920, height=1080):
     return res
 
 
-def bake_bench(gcs, ctx, p, frames=10):
+def bake_bench(gcs, ctx, p, frames=20):
     """simulation.bin baking of the benchmark state: the pipelined gcs_bake
     (device packing, copies on a second stream, writer thread) against the
     reference Bake loop's shape run through the same engine (step, read the

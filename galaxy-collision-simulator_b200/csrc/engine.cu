@@ -78,6 +78,13 @@ struct gcs_ctx {
     unsigned long long* render_acc = nullptr;
     uint8_t* render_rgba = nullptr;
     int64_t render_pixels_cap = 0;
+    // bake: two pinned frame buffers (bake_frames_cap records each), a copy
+    // stream and its events, created at the first gcs_bake and kept
+    PlaybackStar* bake_host[2] = {nullptr, nullptr};
+    int64_t bake_frames_cap = 0;
+    cudaStream_t bake_stream = nullptr;
+    cudaEvent_t bake_packed[2] = {nullptr, nullptr};
+    cudaEvent_t bake_copied[2] = {nullptr, nullptr};
     size_t walk_stack_entries = 0;
     int32_t group_width = 32;              // targets per walk group (<= 64; two per lane above 32)
     size_t groups_cap = 0;
@@ -182,6 +189,15 @@ void drop_graphs(gcs_ctx* c) {
 
 void free_all(gcs_ctx* c) {
     drop_graphs(c);
+    if (c->bake_stream) {
+        cudaStreamSynchronize(c->bake_stream);
+        cudaStreamDestroy(c->bake_stream);
+    }
+    for (int b = 0; b < 2; ++b) {
+        if (c->bake_packed[b]) cudaEventDestroy(c->bake_packed[b]);
+        if (c->bake_copied[b]) cudaEventDestroy(c->bake_copied[b]);
+        if (c->bake_host[b]) cudaFreeHost(c->bake_host[b]);
+    }
     void* ptrs[] = {c->pos[0], c->pos[1], c->vel[0], c->vel[1], c->acc, c->keys[0], c->keys[1],
                     c->idx[0], c->idx[1], c->tr, c->bd, c->wn, c->com64, c->leaf_parent, c->seg_off,
                     c->seg_id, c->groups, c->chunks, c->seg_bounds, c->staging, c->pb_staging,
@@ -1125,15 +1141,28 @@ extern "C" int gcs_bake(gcs_ctx* c, const gcs_params* p, int32_t frames, const c
     cudaSetDevice(c->device);
     const int64_t n = c->n;
     const size_t bytes = sizeof(PlaybackStar) * (size_t)n;
-    PlaybackStar* host[2] = {nullptr, nullptr};
-    cudaStream_t copy = nullptr;
-    cudaEvent_t packed[2] = {nullptr, nullptr}, copied[2] = {nullptr, nullptr};
-    bool ok = cudaMallocHost(reinterpret_cast<void**>(&host[0]), bytes > 0 ? bytes : 1) == cudaSuccess &&
-              cudaMallocHost(reinterpret_cast<void**>(&host[1]), bytes > 0 ? bytes : 1) == cudaSuccess &&
-              cudaStreamCreateWithFlags(&copy, cudaStreamNonBlocking) == cudaSuccess;
-    for (int b = 0; b < 2 && ok; ++b)
-        ok = cudaEventCreateWithFlags(&packed[b], cudaEventDisableTiming) == cudaSuccess &&
-             cudaEventCreateWithFlags(&copied[b], cudaEventDisableTiming) == cudaSuccess;
+    // pinned buffers, copy stream and events live with the context
+    bool ok = true;
+    if (!c->bake_stream) {
+        ok = cudaStreamCreateWithFlags(&c->bake_stream, cudaStreamNonBlocking) == cudaSuccess;
+        for (int b = 0; b < 2 && ok; ++b)
+            ok = cudaEventCreateWithFlags(&c->bake_packed[b], cudaEventDisableTiming) == cudaSuccess &&
+                 cudaEventCreateWithFlags(&c->bake_copied[b], cudaEventDisableTiming) == cudaSuccess;
+    }
+    if (ok && n > c->bake_frames_cap) {
+        for (int b = 0; b < 2; ++b) {
+            if (c->bake_host[b]) cudaFreeHost(c->bake_host[b]);
+            c->bake_host[b] = nullptr;
+        }
+        c->bake_frames_cap = 0;
+        ok = cudaMallocHost(reinterpret_cast<void**>(&c->bake_host[0]), bytes) == cudaSuccess &&
+             cudaMallocHost(reinterpret_cast<void**>(&c->bake_host[1]), bytes) == cudaSuccess;
+        if (ok) c->bake_frames_cap = n;
+    }
+    PlaybackStar* const host[2] = {c->bake_host[0], c->bake_host[1]};
+    const cudaStream_t copy = c->bake_stream;
+    cudaEvent_t* const packed = c->bake_packed;
+    cudaEvent_t* const copied = c->bake_copied;
     BakeWriter W;
     std::thread writer;
     if (ok) {
@@ -1206,15 +1235,7 @@ extern "C" int gcs_bake(gcs_ctx* c, const gcs_params* p, int32_t frames, const c
         rc = GCS_ERR_ARG;
         c->last_error = "bake: closing the output failed";
     }
-    if (copy) {
-        cudaStreamSynchronize(copy);
-        cudaStreamDestroy(copy);
-    }
-    for (int b = 0; b < 2; ++b) {
-        if (packed[b]) cudaEventDestroy(packed[b]);
-        if (copied[b]) cudaEventDestroy(copied[b]);
-        if (host[b]) cudaFreeHost(host[b]);
-    }
+    if (copy) cudaStreamSynchronize(copy);
     if (!rc) rc = gcs_synchronize(c);
     if (seconds) *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     return rc;

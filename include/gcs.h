@@ -299,8 +299,9 @@ int64_t gcs_context_bytes(int64_t capacity, int32_t max_segments, int32_t device
  * appended to with append = 1): the reference's Bake loop (main.cpp:119-297).
  * Frames are packed on the device, copied into two pinned buffers on a
  * second stream while the next step computes, and written by a writer
- * thread in order.  Returns when every frame is on disk; seconds (may be
- * NULL) receives the wall time. */
+ * thread in order (the pinned buffers and the stream are created at the
+ * first call and kept by the context).  Returns when every frame has been
+ * written; seconds (may be NULL) receives the wall time. */
 int gcs_bake(gcs_ctx* ctx, const gcs_params* p, int32_t frames, const char* path, int32_t append,
              double* seconds);
 
