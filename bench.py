@@ -66,6 +66,8 @@ def parse():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-render", action="store_true")
     ap.add_argument("--no-bake", action="store_true")
+    ap.add_argument("--shard", action="store_true",
+                    help="one scenario stepped across the ranks (strong scaling) instead of one per rank")
     ap.add_argument("--batched-count", type=int, default=256)
     ap.add_argument("--batched-steps", type=int, default=10)
     ap.add_argument("--no-served", action="store_true")
@@ -207,6 +209,32 @@ class ClockSampler:
                     reasons.add(name)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi, 200 ms"}
+
+
+def shard_slices(n, world, align=64):
+    """Slices of n sorted particles over `world` ranks for one scenario stepped
+    across devices: every slice is L = ceil(n / world) rounded up to `align`
+    particles long (so its bounds are walk-group starts for group widths that
+    divide `align`), the last ones cut at n.  Returns (L, [(first, count)])."""
+    per = -(-n // world)
+    length = -(-per // align) * align
+    out = []
+    for r in range(world):
+        a = min(r * length, n)
+        out.append((a, min((r + 1) * length, n) - a))
+    return length, out
+
+
+def allgather_slices(dist, full, length, rank):
+    """Every rank's rows [r * length, (r + 1) * length) of `full` (world * length
+    rows) copied to every rank, in place (NCCL), or through a list of chunks
+    where the backend has no in-place all-gather."""
+    mine = full[rank * length:(rank + 1) * length]
+    if full.is_cuda:
+        dist.all_gather_into_tensor(full, mine)
+    else:
+        chunks = list(full.split(length))
+        dist.all_gather(chunks, mine.clone())
 
 
 def replica_throughput(n_local, steps, t_local_s, dist=None, device="cpu"):
@@ -435,6 +463,84 @@ def bake_bench(gcs, ctx, p, frames=20):
     return out
 
 
+def run_sharded(args, gcs, torch, dist, rank, world, local):
+    """--shard: ONE 1M-particle scenario stepped across the ranks.  Every rank
+    runs bounds, sort, build and aggregation over all particles (the same
+    order and tree everywhere), walks and kicks/drifts its slice, and the
+    slices of the position and velocity arrays are all-gathered (NCCL) after
+    each step; the state stays the single-device step's.  Strong scaling:
+    value = particles x steps / the slowest rank's time."""
+    stars = gcs.collision_equal(*counts_for(args.n), seed=0)
+    n = len(stars)
+    length, slices = shard_slices(n, world, 64)
+    first, count = slices[rank]
+    stream = torch.cuda.current_stream()
+    ctx = gcs.Context(max(n, world * length), device=local)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.set_segments([n])
+    ctx.upload(stars)
+    if args.leaf > 0 and args.batch > 0:
+        p, width = make_params(gcs, args.leaf, args.batch), 32
+    else:
+        q = make_params(gcs, 32, 0)
+        q.tune_leaf_min = 4
+        p, _ = ctx.autotune(q)
+        width = ctx.group_width
+    if dist is not None:  # every rank steps with rank 0's settings
+        obj = [(p.leaf_size, p.walk_batch, p.walk_blocks_per_sm, width)]
+        dist.broadcast_object_list(obj, src=0)
+        leaf, batch, bps, width = obj[0]
+        p = make_params(gcs, leaf, batch)
+        p.walk_blocks_per_sm = bps
+    ctx.set_group_width(width)
+    ctx.upload(stars)
+    ctx.set_step_range(first, count)
+
+    def step():
+        ctx.step(p)
+        if dist is not None:
+            for which in (gcs.BUF_POS, gcs.BUF_VEL):
+                allgather_slices(dist, ctx.device_tensor(which, torch, rows=world * length), length, rank)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    clocks = sampler.stop()
+    status = ctx.device_status()
+    if status:
+        raise RuntimeError("device status word 0x%x after the sharded steps" % status)
+    t_ms = ev0.elapsed_time(ev1)
+    if dist is not None:
+        tt = torch.tensor([t_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_ms = float(tt.item())
+    ctx.close()
+    line = {"metric": "particle-steps/s", "value": n * args.steps / (t_ms / 1e3), "unit": "particle-steps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms / args.steps,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded two-galaxy initial conditions, seed 0 on every rank)",
+            "config": {"workload": WORKLOAD, "particles": n, "leaf_size": p.leaf_size, "walk_batch": p.walk_batch,
+                       "group_width": width, "parallelism": "target-sharded x%d (slices of %d particles, "
+                       "position/velocity all-gather per step)" % (world, length)},
+            "clocks": clocks, "device_status": status}
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
 def batched_bench(gcs, torch, args):
     """256 uneven scenarios: all advanced together (segments of one context,
     one launch per stage, graph-captured step) versus the same scenarios one
@@ -649,6 +755,12 @@ def main():
     def barrier():
         if dist is not None:
             dist.barrier()
+
+    if args.shard:
+        rc = run_sharded(args, gcs, torch, dist, rank, world, local)
+        if dist is not None:
+            dist.destroy_process_group()
+        return rc
 
     stars = gcs.collision_equal(*counts_for(args.n), seed=rank)
     n = len(stars)

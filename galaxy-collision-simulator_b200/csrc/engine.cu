@@ -87,6 +87,10 @@ struct gcs_ctx {
     cudaEvent_t bake_copied[2] = {nullptr, nullptr};
     size_t walk_stack_entries = 0;
     int32_t group_width = 32;              // targets per walk group (<= 64; two per lane above 32)
+    // particles the walk and the kick/drift cover (sorted order; count < 0:
+    // all): one rank's slice when one scenario is stepped across devices
+    int64_t range_first = 0;
+    int64_t range_count = -1;
     size_t groups_cap = 0;
     bool count_walk = false;
 
@@ -239,12 +243,30 @@ WalkNodeParams walk_node_params(const gcs_ctx* c, const gcs_params* p) {
 
 // Walk work units: runs of <= group_width consecutive particles that never
 // straddle a segment, so a segment's groups are the same alone or batched.
+// First particle and count the walk and the kick/drift cover.
+int64_t range_first(const gcs_ctx* c) { return c->range_count < 0 ? 0 : std::min<int64_t>(c->range_first, c->n); }
+int64_t range_count(const gcs_ctx* c) {
+    const int64_t f = range_first(c);
+    return c->range_count < 0 ? c->n : std::max<int64_t>(0, std::min<int64_t>(c->range_count, c->n - f));
+}
+
+// A range boundary must be the end of the particles or the first particle
+// of a walk group (so that no group is split between ranges).
+bool range_boundary_ok(const gcs_ctx* c, int64_t b) {
+    if (b == c->n) return true;
+    for (int s = 0; s < c->nseg; ++s)
+        if (b >= c->h_seg_off[s] && b < c->h_seg_off[s + 1]) return (b - c->h_seg_off[s]) % c->group_width == 0;
+    return false;
+}
+
 int upload_groups(gcs_ctx* c) {
     std::vector<WalkGroup> groups;
     groups.reserve((size_t)(c->n / c->group_width + c->nseg + 1));
+    const int64_t rf = range_first(c), rl = rf + range_count(c);
     for (int s = 0; s < c->nseg; ++s) {
         const int64_t a = c->h_seg_off[s], e = c->h_seg_off[s + 1];
         for (int64_t g = a; g < e; g += c->group_width) {
+            if (g < rf || g >= rl) continue;  // outside this context's step range
             WalkGroup w;
             w.start = (int32_t)g;
             w.count = (int32_t)std::min<int64_t>(c->group_width, e - g);
@@ -340,9 +362,12 @@ static int run_stage(gcs_ctx* c, const gcs_params* p, int stage) {
                         c->count_walk ? c->counts : nullptr, c->walk_stack, c->walk_stack_entries, st);
             return check_launch(c, "walk");
         }
-        case GCS_STAGE_INTEGRATE:
-            launch_integrate(c->pos[c->cur], c->vel[c->cur], c->acc, p->dt, p->recolor, c->n, st);
+        case GCS_STAGE_INTEGRATE: {
+            const int64_t f = range_first(c);
+            launch_integrate(c->pos[c->cur] + f, c->vel[c->cur] + f, c->acc + f, p->dt, p->recolor, range_count(c),
+                             st);
             return check_launch(c, "integrate");
+        }
         default:
             c->last_error = "unknown stage";
             return GCS_ERR_ARG;
@@ -595,6 +620,8 @@ static int apply_layout(gcs_ctx* c, int32_t num_segments, const int64_t* counts)
     c->n_internal = (int32_t)(n - num_segments);
     c->n_chunks = (int)chunks.size();
     c->tree_gen++;  // the tree (and its walk records) belong to the old layout
+    c->range_first = 0;  // a new layout steps every particle until a range is set again
+    c->range_count = -1;
     drop_graphs(c);
     return upload_groups(c);
 }
@@ -658,7 +685,14 @@ int64_t gcs_segment_offset(const gcs_ctx* c, int32_t segment) {
 
 int gcs_set_group_width(gcs_ctx* c, int32_t width) {
     if (!c || width < kMinGroupWidth || width > kGroupSize) return GCS_ERR_ARG;
+    const int32_t old = c->group_width;
     c->group_width = width;
+    if (c->range_count >= 0 &&
+        (!range_boundary_ok(c, c->range_first) || !range_boundary_ok(c, c->range_first + c->range_count))) {
+        c->group_width = old;
+        c->last_error = "group width would split a walk group across the step range";
+        return GCS_ERR_STATE;
+    }
     drop_graphs(c);
     return upload_groups(c);
 }
@@ -805,8 +839,37 @@ int gcs_compute_accels(gcs_ctx* c, const gcs_params* p) {
 
 int gcs_kick(gcs_ctx* c, float dt) {
     if (!c) return GCS_ERR_ARG;
-    launch_kick(c->vel[c->cur], c->acc, dt, c->n, c->stream);
+    const int64_t f = range_first(c);
+    launch_kick(c->vel[c->cur] + f, c->acc + f, dt, range_count(c), c->stream);
     return check_launch(c, "kick");
+}
+
+int gcs_set_step_range(gcs_ctx* c, int64_t first, int64_t count) {
+    if (!c) return GCS_ERR_ARG;
+    if (count < 0) {
+        c->range_first = 0;
+        c->range_count = -1;
+    } else {
+        if (first < 0 || first > c->n || count > c->n - first || !range_boundary_ok(c, first) ||
+            !range_boundary_ok(c, first + count)) {
+            c->last_error = "step range: bounds must be walk-group starts within the particles";
+            return GCS_ERR_ARG;
+        }
+        c->range_first = first;
+        c->range_count = count;
+    }
+    drop_graphs(c);
+    return upload_groups(c);
+}
+
+void* gcs_device_array(gcs_ctx* c, int32_t which) {
+    if (!c) return nullptr;
+    switch (which) {
+        case GCS_BUF_POS: return c->pos[c->cur];
+        case GCS_BUF_VEL: return c->vel[c->cur];
+        case GCS_BUF_ACCEL: return c->acc;
+        default: return nullptr;
+    }
 }
 
 int gcs_run_stages(gcs_ctx* c, const gcs_params* p, int32_t first, int32_t last) {

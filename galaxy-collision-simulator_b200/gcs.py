@@ -132,6 +132,8 @@ def lib() -> C.CDLL:
         "gcs_device_bytes": (i64, [P]),
         "gcs_context_bytes": (i64, [i64, i32, i32]),
         "gcs_bake": (C.c_int, [P, C.POINTER(Params), i32, C.c_char_p, i32, C.POINTER(C.c_double)]),
+        "gcs_set_step_range": (C.c_int, [P, i64, i64]),
+        "gcs_device_array": (P, [P, i32]),
         "gcs_camera_reference": (None, [C.POINTER(Camera)]),
         "gcs_camera_matrices": (C.c_int, [C.POINTER(Camera), i32, i32, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
         "gcs_render_frame": (C.c_int, [P, C.POINTER(Camera), i32, i32, i32, P, i32]),
@@ -363,6 +365,31 @@ class Context:
         self.check(self.L.gcs_count_interactions(self._h, C.byref(p), out))
         r = tuple(int(x) for x in out)
         return r if warp_evals else r[:2]
+
+    def set_step_range(self, first: int, count: int) -> None:
+        """Walk and kick/drift only the sorted particles [first, first + count)
+        (count < 0: all); see gcs_set_step_range."""
+        self.check(self.L.gcs_set_step_range(self._h, first, count))
+
+    def device_array(self, which: int) -> int:
+        """Device address of the current POS / VEL / ACCEL array (float4 rows)."""
+        ptr = self.L.gcs_device_array(self._h, which)
+        if not ptr:
+            raise GcsError("gcs_device_array: no such array")
+        return int(ptr)
+
+    def device_tensor(self, which: int, torch, rows: int | None = None):
+        """A torch float32 tensor [rows, 4] viewing the current POS / VEL /
+        ACCEL array in place (no copy); valid until the next step."""
+        rows = self.n if rows is None else rows
+
+        class _View:
+            pass
+
+        v = _View()
+        v.__cuda_array_interface__ = {"shape": (rows, 4), "typestr": "<f4",
+                                      "data": (self.device_array(which), False), "version": 3}
+        return torch.as_tensor(v, device="cuda")
 
     def bake(self, p: Params, frames: int, path: str, append: bool = False) -> float:
         """`frames` steps, each written as a simulation.bin frame to `path`;

@@ -118,6 +118,26 @@ int32_t gcs_num_segments(const gcs_ctx* ctx);
 int gcs_set_group_width(gcs_ctx* ctx, int32_t width);
 int32_t gcs_group_width(const gcs_ctx* ctx);
 
+/* ---- one scenario across devices -----------------------------------------
+ * Every rank of a multi-GPU job holds the whole scenario and runs the same
+ * bounds, sort, build and aggregation, which give the same sorted order and
+ * tree everywhere; each rank then walks and kicks/drifts only its slice of
+ * the sorted particles, and an all-gather of the slices of the position and
+ * velocity arrays (gcs_device_array) completes the step.  The result is the
+ * single-device step, bit for bit.  (The reference steps one scenario on one
+ * device; this has no counterpart there.) */
+/* Restrict the walk and the kick/drift (gcs_step, the walk and integrate
+ * stages, gcs_kick) to the sorted particles [first, first + count); count < 0
+ * restores every particle.  Both bounds must be the first particle of a walk
+ * group (a multiple of the group width within its segment) or the particle
+ * count.  A layout change resets the range. */
+int gcs_set_step_range(gcs_ctx* ctx, int64_t first, int64_t count);
+/* Device address of the context's current arrays: which = GCS_BUF_POS or
+ * GCS_BUF_VEL (float4 per particle, the state after the last step) or
+ * GCS_BUF_ACCEL; NULL otherwise.  Steps alternate between two position and
+ * velocity arrays, so ask again after every step. */
+void* gcs_device_array(gcs_ctx* ctx, int32_t which);
+
 /* ---- particle data ------------------------------------------------------ */
 /* Copy host Stars into particles [offset, offset+n) (host may be pageable or
  * pinned); the reference's cuda_upload_initial_stars (cuda_engine.cu:342-352). */

@@ -1,0 +1,74 @@
+"""One scenario stepped across devices, emulated on one GPU: two contexts
+hold the same scenario, each walks and kicks/drifts its own slice of the
+sorted particles (gcs_set_step_range), and the slices of the position and
+velocity arrays are exchanged after every step (the all-gather of a
+multi-GPU job, here device-to-device copies through gcs_device_array).
+Both contexts must then hold exactly the single-context state."""
+import numpy as np
+import pytest
+
+from conftest import small_collision
+
+pytestmark = pytest.mark.gpu
+
+
+def _params(gcs):
+    return gcs.reference_params(theta=0.5, epsilon_sq=0.05 ** 2, dt=0.005, leaf_size=4, walk_batch=64,
+                                bounds_mode=gcs.BOUNDS_DEVICE, com_fp64=1)
+
+
+@pytest.mark.parametrize("width,graphs", [(32, False), (64, False), (32, True)])
+def test_two_slices_equal_one_context(gcs_mod, width, graphs):
+    import bench
+    import torch
+    gcs = gcs_mod
+    stars = small_collision(3000, 700, 300, seed=41)  # 8,000 particles
+    n = len(stars)
+    p = _params(gcs)
+    length, slices = bench.shard_slices(n, 2, 64)
+    s = torch.cuda.Stream()
+    with gcs.Context(2 * length) as a, gcs.Context(2 * length) as b, gcs.Context(n) as whole:
+        for ctx, (first, count) in ((a, slices[0]), (b, slices[1])):
+            ctx.set_stream(s.cuda_stream)
+            ctx.set_segments([n])
+            ctx.set_group_width(width)
+            ctx.upload(stars)
+            ctx.set_step_range(first, count)
+            ctx.set_graphs(graphs)
+        whole.set_stream(s.cuda_stream)
+        whole.set_group_width(width)
+        whole.upload(stars)
+        with torch.cuda.stream(s):
+            for _ in range(4):
+                a.step(p)
+                b.step(p)
+                whole.step(p)
+                for which in (gcs.BUF_POS, gcs.BUF_VEL):
+                    ta = a.device_tensor(which, torch)
+                    tb = b.device_tensor(which, torch)
+                    f1, c1 = slices[1]
+                    ta[f1:f1 + c1].copy_(tb[f1:f1 + c1])
+                    tb[:slices[0][1]].copy_(ta[:slices[0][1]])
+        s.synchronize()
+        ref = whole.download().tobytes()
+        assert a.download().tobytes() == ref
+        assert b.download().tobytes() == ref
+        assert a.device_status() == 0 and b.device_status() == 0
+
+
+def test_step_range_bounds_are_checked(gcs_mod):
+    gcs = gcs_mod
+    stars = small_collision(512, 128, 64, seed=42)
+    n = len(stars)
+    with gcs.Context(n) as ctx:
+        ctx.upload(stars)
+        with pytest.raises(gcs.GcsError):
+            ctx.set_step_range(17, 64)          # not a group start
+        with pytest.raises(gcs.GcsError):
+            ctx.set_step_range(0, n + 32)       # past the particles
+        ctx.set_step_range(64, n - 64)          # to the end: fine
+        with pytest.raises(gcs.GcsError):
+            ctx.set_group_width(48)             # 64 is not a multiple of 48
+        ctx.set_group_width(16)
+        ctx.set_step_range(0, -1)               # every particle again
+        assert ctx.device_array(gcs.BUF_POS) != ctx.device_array(gcs.BUF_VEL)
