@@ -833,7 +833,8 @@ def main():
     e2e_value, t_e2e, _ = replica_throughput(n, ke, t_e2e, dist, "cuda")
     e2e = {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": 32 * n,
            "d2h_bytes_per_step": 32 * n, "steps": ke,
-           "path": "gcs_upload_stars (pinned Star[] H2D) + gcs_step_host (step, pack, Star[] D2H)"}
+           "path": "gcs_upload_stars (pinned Star[] H2D) + gcs_step_host (step; Star[] D2H of each finished "
+                   "chunk of walk groups, overlapped with the walk)"}
 
     peaks = measured_peaks()
     sm_max = float(peaks.get("sm_max_mhz", 1965.0))

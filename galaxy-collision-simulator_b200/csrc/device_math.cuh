@@ -122,6 +122,28 @@ __device__ __forceinline__ uint32_t recolour(uint32_t tcol, float vx, float vy, 
     return type | (r << 8) | (g << 16) | (b << 24);
 }
 
+// ---- kick/drift of one particle (cuda_engine.cu:164-216) --------------------
+// v += a dt; x += v dt; recolour types 0/2 by speed.  The reference's two
+// statements per axis contract to fma(a, dt, v) and fma(v, dt, x).  The
+// separate integrate kernel and the walk's fused epilogue both call this, so
+// their results are the same bits.
+__device__ __forceinline__ void kick_drift(float4& p, float4& v, float4 a, float dt, int recolor) {
+    v.x = __fmaf_rn(a.x, dt, v.x);
+    v.y = __fmaf_rn(a.y, dt, v.y);
+    v.z = __fmaf_rn(a.z, dt, v.z);
+    p.x = __fmaf_rn(v.x, dt, p.x);
+    p.y = __fmaf_rn(v.y, dt, p.y);
+    p.z = __fmaf_rn(v.z, dt, p.z);
+    if (recolor) v.w = __uint_as_float(recolour(__float_as_uint(v.w), v.x, v.y, v.z));
+}
+
+// ---- Star record (types.h:5-11) as two float4 ------------------------------
+// Star (x,y,z,vx | vy,vz,m,tcol) from pos (x,y,z,m) and vel (vx,vy,vz,tcol).
+__device__ __forceinline__ void store_star(float4* __restrict__ stars, int64_t i, float4 p, float4 v) {
+    stars[2 * i] = make_float4(p.x, p.y, p.z, v.x);
+    stars[2 * i + 1] = make_float4(v.y, v.z, p.w, v.w);
+}
+
 // ---- order-preserving float <-> u32 (for atomicMax-based min/max) ----------
 __device__ __forceinline__ uint32_t float_to_ordered(float f) {
     const uint32_t u = __float_as_uint(f);

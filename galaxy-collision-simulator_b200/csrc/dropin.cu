@@ -120,13 +120,17 @@ float cuda_physics_step(Star* host_stars, int num_stars, float G, float epsilon_
     p.global_min = global_min;
     p.global_max = global_max;
     if (gcs_num_particles(g_ctx) != num_stars) return dt;
-    if (gcs_step(g_ctx, &p) != GCS_OK) return dt;
     if (use_interop && g_vbo_registered) {
         // No graphics stack here: the Stars go to the device buffer a mapped
         // VBO would have received (cuda_engine.cu:427-440), host untouched.
+        if (gcs_step(g_ctx, &p) != GCS_OK) return dt;
         gcs::pack_to_device(g_ctx, g_interop_stars);
     } else if (host_stars) {
-        gcs_download_stars(g_ctx, host_stars, 0, num_stars);
+        // the step with the Star copy (cuda_engine.cu:442-448) overlapped
+        // with the walk
+        gcs_step_host(g_ctx, &p, host_stars);
+    } else {
+        gcs_step(g_ctx, &p);
     }
     return dt;
 }

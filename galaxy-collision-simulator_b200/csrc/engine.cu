@@ -33,6 +33,7 @@ struct gcs_ctx {
     // layout
     int32_t n = 0, nseg = 0, n_internal = 0;
     std::vector<int64_t> h_seg_off;
+    std::vector<int32_t> h_group_start;  // first particle of each walk group (host copy)
     int n_groups = 0, n_chunks = 0;
 
     // device state
@@ -85,6 +86,16 @@ struct gcs_ctx {
     cudaStream_t bake_stream = nullptr;
     cudaEvent_t bake_packed[2] = {nullptr, nullptr};
     cudaEvent_t bake_copied[2] = {nullptr, nullptr};
+    // host step with the Star copy overlapped with the walk (gcs_step_host):
+    // a copy stream, an event after the walk, per-chunk completion flags in
+    // mapped host memory (written by the walk's epilogue) and their device
+    // counters; created at the first such step and kept
+    cudaStream_t star_stream = nullptr;
+    cudaEvent_t star_walked = nullptr;
+    uint32_t* star_flags = nullptr;      // mapped host memory, kMaxStarChunks words
+    uint32_t* star_flags_dev = nullptr;  // its device address
+    uint32_t* star_chunk_done = nullptr;
+    uint32_t star_epoch = 0;
     size_t walk_stack_entries = 0;
     int32_t group_width = 32;              // targets per walk group (<= 64; two per lane above 32)
     // particles the walk and the kick/drift cover (sorted order; count < 0:
@@ -202,11 +213,17 @@ void free_all(gcs_ctx* c) {
         if (c->bake_copied[b]) cudaEventDestroy(c->bake_copied[b]);
         if (c->bake_host[b]) cudaFreeHost(c->bake_host[b]);
     }
+    if (c->star_stream) {
+        cudaStreamSynchronize(c->star_stream);
+        cudaStreamDestroy(c->star_stream);
+    }
+    if (c->star_walked) cudaEventDestroy(c->star_walked);
+    if (c->star_flags) cudaFreeHost(c->star_flags);
     void* ptrs[] = {c->pos[0], c->pos[1], c->vel[0], c->vel[1], c->acc, c->keys[0], c->keys[1],
                     c->idx[0], c->idx[1], c->tr, c->bd, c->wn, c->com64, c->leaf_parent, c->seg_off,
                     c->seg_id, c->groups, c->chunks, c->seg_bounds, c->staging, c->pb_staging,
                     c->scratch, c->status, c->diag, c->targets, c->direct_out, c->counts,
-                    c->walk_stack, c->render_acc, c->render_rgba};
+                    c->walk_stack, c->render_acc, c->render_rgba, c->star_chunk_done};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }
@@ -284,6 +301,8 @@ int upload_groups(gcs_ctx* c) {
     GCS_CUDA(c, cudaMemcpyAsync(c->groups, groups.data(), sizeof(WalkGroup) * groups.size(),
                                 cudaMemcpyHostToDevice, c->stream));
     c->n_groups = (int)groups.size();
+    c->h_group_start.resize(groups.size());
+    for (size_t g = 0; g < groups.size(); ++g) c->h_group_start[g] = groups[g].start;
     return GCS_OK;
 }
 
@@ -292,6 +311,32 @@ int upload_groups(gcs_ctx* c) {
 // ---------------------------------------------------------------------------
 // stage sequence
 // ---------------------------------------------------------------------------
+// The walk stage, with an optional epilogue (the fused kick/drift and Star
+// records of the overlapped host step).
+static int walk_stage(gcs_ctx* c, const gcs_params* p, const WalkEpilogue& ep) {
+    cudaStream_t st = c->stream;
+    const Layout L = layout_of(c);
+    const ScratchLayout sl = scratch_layout(c->max_segments, c->n, c->nseg);
+    WalkParams wp;
+    wp.G = p->G;
+    wp.eps2 = p->epsilon_sq;
+    wp.theta2 = p->theta * p->theta;
+    wp.leaf_size = p->leaf_size;
+    wp.batch = p->walk_batch > 0 ? p->walk_batch : default_walk_batch();
+    wp.with_potential = p->with_potential ? 1 : 0;
+    const WalkNodeParams wnp = walk_node_params(c, p);
+    if (c->wn_gen != c->tree_gen || c->wn_G != wnp.G || c->wn_L != wnp.leaf_size) {
+        launch_walk_nodes(L, c->tr, wnp, c->status, st);
+        c->wn_gen = c->tree_gen;
+        c->wn_G = wnp.G;
+        c->wn_L = wnp.leaf_size;
+    }
+    launch_walk(L, wp, c->pos[c->cur], c->wn, c->groups, c->n_groups, c->group_width > 32 ? 2 : 1, c->acc,
+                scratch_at<uint32_t>(c, sl.walk_q), c->status, p->walk_blocks_per_sm, c->sm_count,
+                c->count_walk ? c->counts : nullptr, c->walk_stack, c->walk_stack_entries, st, ep);
+    return check_launch(c, "walk");
+}
+
 static int run_stage(gcs_ctx* c, const gcs_params* p, int stage) {
     cudaStream_t st = c->stream;
     const Layout L = layout_of(c);
@@ -342,26 +387,8 @@ static int run_stage(gcs_ctx* c, const gcs_params* p, int stage) {
             c->wn_L = wnp.leaf_size;
             return check_launch(c, "aggregate");
         }
-        case GCS_STAGE_WALK: {
-            WalkParams wp;
-            wp.G = p->G;
-            wp.eps2 = p->epsilon_sq;
-            wp.theta2 = p->theta * p->theta;
-            wp.leaf_size = p->leaf_size;
-            wp.batch = p->walk_batch > 0 ? p->walk_batch : default_walk_batch();
-            wp.with_potential = p->with_potential ? 1 : 0;
-            const WalkNodeParams wnp = walk_node_params(c, p);
-            if (c->wn_gen != c->tree_gen || c->wn_G != wnp.G || c->wn_L != wnp.leaf_size) {
-                launch_walk_nodes(L, c->tr, wnp, c->status, st);
-                c->wn_gen = c->tree_gen;
-                c->wn_G = wnp.G;
-                c->wn_L = wnp.leaf_size;
-            }
-            launch_walk(L, wp, c->pos[c->cur], c->wn, c->groups, c->n_groups, c->group_width > 32 ? 2 : 1, c->acc,
-                        scratch_at<uint32_t>(c, sl.walk_q), c->status, p->walk_blocks_per_sm, c->sm_count,
-                        c->count_walk ? c->counts : nullptr, c->walk_stack, c->walk_stack_entries, st);
-            return check_launch(c, "walk");
-        }
+        case GCS_STAGE_WALK:
+            return walk_stage(c, p, WalkEpilogue());
         case GCS_STAGE_INTEGRATE: {
             const int64_t f = range_first(c);
             launch_integrate(c->pos[c->cur] + f, c->vel[c->cur] + f, c->acc + f, p->dt, p->recolor, range_count(c),
@@ -825,8 +852,104 @@ int gcs_set_graphs(gcs_ctx* c, int32_t enable) {
 
 int32_t gcs_graph_builds(const gcs_ctx* c) { return c ? c->graph_builds : 0; }
 
+// Resources of the overlapped host step, created at its first use.
+static int ensure_star_pipeline(gcs_ctx* c) {
+    if (!c->star_stream) GCS_CUDA(c, cudaStreamCreateWithFlags(&c->star_stream, cudaStreamNonBlocking));
+    if (!c->star_walked) GCS_CUDA(c, cudaEventCreateWithFlags(&c->star_walked, cudaEventDisableTiming));
+    if (!c->star_flags) {
+        GCS_CUDA(c, cudaHostAlloc(reinterpret_cast<void**>(&c->star_flags), sizeof(uint32_t) * kMaxStarChunks,
+                                  cudaHostAllocMapped));
+        memset(c->star_flags, 0, sizeof(uint32_t) * kMaxStarChunks);
+        GCS_CUDA(c, cudaHostGetDevicePointer(reinterpret_cast<void**>(&c->star_flags_dev), c->star_flags, 0));
+    }
+    if (!c->star_chunk_done) {
+        const int rc = dalloc(c, &c->star_chunk_done, kMaxStarChunks);
+        if (rc) return rc;
+    }
+    return GCS_OK;
+}
+
+// One step whose Stars land in `host`, with the copy overlapped with the
+// walk: the walk's epilogue applies the kick/drift out of place and writes
+// each group's Star records; the host copies every chunk of groups (up to
+// kMaxStarChunks per step) as soon as its flag arrives.  The result is the
+// same bits as the plain stage sequence followed by gcs_download_stars.  A
+// step range (one slice of the scenario) takes that plain sequence.
+static int step_host_overlapped(gcs_ctx* c, const gcs_params* p, Star* host) {
+    int rc = run_stages(c, p, GCS_STAGE_BOUNDS, GCS_STAGE_AGGREGATE);
+    if (rc) return rc;
+    rc = ensure_star_pipeline(c);
+    if (rc) return rc;
+    const int ng = c->n_groups;
+    const int gpc = (ng + kMaxStarChunks - 1) / kMaxStarChunks;
+    const int chunks = (ng + gpc - 1) / gpc;
+    if (++c->star_epoch == 0) c->star_epoch = 1;
+    const uint32_t epoch = c->star_epoch;
+    GCS_CUDA(c, cudaMemsetAsync(c->star_chunk_done, 0, sizeof(uint32_t) * (size_t)chunks, c->stream));
+    WalkEpilogue ep;
+    ep.vel_in = c->vel[c->cur];
+    ep.pos_out = c->pos[c->cur ^ 1];
+    ep.vel_out = c->vel[c->cur ^ 1];
+    ep.stars = reinterpret_cast<float4*>(c->staging);
+    ep.dt = p->dt;
+    ep.recolor = p->recolor;
+    ep.groups_per_chunk = gpc;
+    ep.chunk_done = c->star_chunk_done;
+    ep.host_flags = c->star_flags_dev;
+    ep.epoch = epoch;
+    rc = walk_stage(c, p, ep);
+    if (rc) return rc;
+    c->cur ^= 1;  // the epilogue wrote the stepped state into the other arrays
+    GCS_CUDA(c, cudaEventRecord(c->star_walked, c->stream));
+    // Copy each chunk once its flag is up; when the walk has finished, copy
+    // what is left (a chunk that was never signalled is reported).
+    bool missing = false;
+    for (int k = 0; k < chunks && !rc; ++k) {
+        const int64_t first = c->h_group_start[(size_t)k * gpc];
+        const int64_t end = (int64_t)(k + 1) * gpc < ng ? c->h_group_start[(size_t)(k + 1) * gpc] : c->n;
+        for (uint32_t polls = 1;; ++polls) {
+            if (__atomic_load_n(c->star_flags + k, __ATOMIC_ACQUIRE) == epoch) break;
+            if ((polls & 63u) == 0u) {
+                const cudaError_t q = cudaEventQuery(c->star_walked);
+                if (q == cudaSuccess) {
+                    if (__atomic_load_n(c->star_flags + k, __ATOMIC_ACQUIRE) != epoch) missing = true;
+                    break;
+                }
+                if (q != cudaErrorNotReady) {
+                    set_error(c, "walk", q);
+                    rc = GCS_ERR_CUDA;
+                    break;
+                }
+            }
+        }
+        if (rc) break;
+        const cudaError_t e = cudaMemcpyAsync(host + first, c->staging + first, sizeof(Star) * (size_t)(end - first),
+                                              cudaMemcpyDeviceToHost, c->star_stream);
+        if (e != cudaSuccess) {
+            set_error(c, "cudaMemcpyAsync (Stars)", e);
+            rc = GCS_ERR_CUDA;
+        }
+    }
+    // no copy into the caller's buffer may outlive this call
+    const cudaError_t e1 = cudaStreamSynchronize(c->star_stream);
+    const cudaError_t e2 = cudaStreamSynchronize(c->stream);
+    if (rc) return rc;
+    if (e1 != cudaSuccess || e2 != cudaSuccess) {
+        set_error(c, "cudaStreamSynchronize (host step)", e1 != cudaSuccess ? e1 : e2);
+        return GCS_ERR_CUDA;
+    }
+    if (missing) {
+        c->last_error = "host step: a chunk of Star records was not signalled by the walk";
+        return GCS_ERR_STATE;
+    }
+    return GCS_OK;
+}
+
 int gcs_step_host(gcs_ctx* c, const gcs_params* p, Star* host) {
     if (!c || !host) return GCS_ERR_ARG;
+    cudaSetDevice(c->device);
+    if (c->range_count < 0 && c->n_groups > 0 && c->n > 0)
+        return step_host_overlapped(c, p, host);
     int rc = run_stages(c, p, GCS_STAGE_BOUNDS, GCS_STAGE_INTEGRATE);
     if (rc) return rc;
     return gcs_download_stars(c, host, 0, c->n);

@@ -137,11 +137,34 @@ void launch_walk_nodes(const Layout& L, const BvhNodeTraverse* tr, WalkNodeParam
 constexpr int kWalkGlobalStack = 8192;
 constexpr int kWalkMaxBatch = 64;  // nodes popped per walk round
 // targets_per_lane: 1 for groups of <= 32 targets, 2 for groups of <= 64.
+// Optional epilogue of the walk: each warp, once its group's accelerations
+// are written, applies the kick/drift to the group's particles out of place
+// (pos/vel_in -> pos_out/vel_out, so the walk's other warps keep reading the
+// step's positions) and writes their Star records.  Groups are counted per
+// chunk of `groups_per_chunk` consecutive groups; the warp that completes a
+// chunk stores `epoch` into host_flags[chunk] (mapped host memory, after a
+// system-scope fence), so the host can copy that chunk's Stars while the
+// walk continues.  vel_in == nullptr: no epilogue.  chunk_done must be zero
+// at launch.
+struct WalkEpilogue {
+    const float4* vel_in = nullptr;
+    float4* pos_out = nullptr;
+    float4* vel_out = nullptr;
+    float4* stars = nullptr;  // Star records as float4 pairs
+    float dt = 0.0f;
+    int32_t recolor = 0;
+    int32_t groups_per_chunk = 1;
+    uint32_t* chunk_done = nullptr;
+    uint32_t* host_flags = nullptr;
+    uint32_t epoch = 0;
+};
+constexpr int kMaxStarChunks = 32;
+
 void launch_walk(const Layout& L, const WalkParams& wp, const float4* pos,
                  const WalkNode* wn, const WalkGroup* groups, int n_groups, int targets_per_lane,
                  float4* acc, uint32_t* queue, uint32_t* status, int blocks_per_sm,
                  int sm_count, unsigned long long* counts, int2* gstack, size_t gstack_entries,
-                 cudaStream_t st);
+                 cudaStream_t st, const WalkEpilogue& ep = WalkEpilogue());
 int walk_max_blocks_per_sm(int batch, int with_potential, int targets_per_lane);
 // Persistent walk grid (blocks) for n_groups groups, and the global stack
 // entries that grid needs.

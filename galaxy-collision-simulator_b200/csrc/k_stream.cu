@@ -60,10 +60,7 @@ __global__ void pack_stars_kernel(const float4* __restrict__ pos, const float4* 
                                   float4* __restrict__ stars, int64_t n) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
-        const float4 p = pos[i];
-        const float4 v = vel[i];
-        stars[2 * i] = make_float4(p.x, p.y, p.z, v.x);
-        stars[2 * i + 1] = make_float4(v.y, v.z, p.w, v.w);
+        store_star(stars, i, pos[i], vel[i]);
     }
 }
 
@@ -196,9 +193,8 @@ __global__ void gather_kernel(const uint32_t* __restrict__ idx, const float4* __
     }
 }
 
-// v += a dt; x += v dt; recolour types 0/2 by speed (cuda_engine.cu:164-216).
-// The reference's two statements per axis contract to fma(a, dt, v) and
-// fma(v, dt, x).
+// v += a dt; x += v dt; recolour types 0/2 by speed (kick_drift,
+// cuda_engine.cu:164-216), in place.
 __global__ void integrate_kernel(float4* __restrict__ pos, float4* __restrict__ vel,
                                  const float4* __restrict__ acc, float dt, int recolor, int64_t n) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
@@ -206,13 +202,7 @@ __global__ void integrate_kernel(float4* __restrict__ pos, float4* __restrict__ 
         const float4 a = __ldg(acc + i);
         float4 v = vel[i];
         float4 p = pos[i];
-        v.x = __fmaf_rn(a.x, dt, v.x);
-        v.y = __fmaf_rn(a.y, dt, v.y);
-        v.z = __fmaf_rn(a.z, dt, v.z);
-        p.x = __fmaf_rn(v.x, dt, p.x);
-        p.y = __fmaf_rn(v.y, dt, p.y);
-        p.z = __fmaf_rn(v.z, dt, p.z);
-        if (recolor) v.w = __uint_as_float(recolour(__float_as_uint(v.w), v.x, v.y, v.z));
+        kick_drift(p, v, a, dt, recolor);
         vel[i] = v;
         pos[i] = p;
     }

@@ -50,6 +50,13 @@
 // written out of bounds); a walk that pops more nodes than the tree holds
 // stops with GCS_DEV_TREE_MALFORMED.  The work queue resets itself: the last
 // warp to find it empty zeroes it.
+//
+// With an epilogue (WalkEpilogue), a warp that has written its group's
+// accelerations also applies the step's kick/drift to those particles, out of
+// place, and writes their Star records; the warp that completes a chunk of
+// groups raises that chunk's flag in mapped host memory.  The host copies
+// finished chunks to its Star array while the walk is still running (the
+// reference copies all Stars after the step, cuda_engine.cu:442-448).
 #include <algorithm>
 
 #include "gcs_internal.h"
@@ -274,7 +281,7 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
             const WalkNode* __restrict__ wn, const WalkGroup* __restrict__ groups,
             int n_groups, float4* __restrict__ acc, uint32_t* __restrict__ queue,
             uint32_t* __restrict__ status, unsigned long long* __restrict__ counts,
-            typename EntryOf<T>::type* __restrict__ gstack, int gstack_cap) {
+            typename EntryOf<T>::type* __restrict__ gstack, int gstack_cap, WalkEpilogue ep) {
     using Smem = WarpSmem<H, T>;
     using Entry = typename Smem::Entry;
     extern __shared__ __align__(16) unsigned char walk_smem[];
@@ -625,11 +632,37 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
         }
         if (nsrc > 0) flush_sources<H, T, kPot, kCount>(W, nsrc, lane, lane_bit, pos, G, X, e2, leaf_thr, A, WC);
 #pragma unroll
-        for (int t = 0; t < T; ++t)
-            if (valid[t])
-                acc[grp.start + lane + 32 * t] =
-                    make_float4(__fadd_rn(A[t].ax.x, A[t].ax.y), __fadd_rn(A[t].ay.x, A[t].ay.y),
-                                __fadd_rn(A[t].az.x, A[t].az.y), __fadd_rn(A[t].pot.x, A[t].pot.y));
+        for (int t = 0; t < T; ++t) {
+            if (!valid[t]) continue;
+            const int64_t i = grp.start + lane + 32 * t;
+            const float4 a = make_float4(__fadd_rn(A[t].ax.x, A[t].ax.y), __fadd_rn(A[t].ay.x, A[t].ay.y),
+                                         __fadd_rn(A[t].az.x, A[t].az.y), __fadd_rn(A[t].pot.x, A[t].pot.y));
+            acc[i] = a;
+            if (ep.vel_in) {
+                // the step's kick/drift of this target, out of place, and its Star
+                float4 p = __ldg(pos + i);
+                float4 v = __ldg(ep.vel_in + i);
+                kick_drift(p, v, a, ep.dt, ep.recolor);
+                ep.pos_out[i] = p;
+                ep.vel_out[i] = v;
+                store_star(ep.stars, i, p, v);
+            }
+        }
+        if (ep.vel_in) {
+            // count the group in its chunk; the warp that completes the chunk
+            // tells the host (every warp fences before counting, so a chunk
+            // seen complete has all of its records written)
+            __syncwarp();
+            if (lane == 0) {
+                __threadfence();
+                const int k = g / ep.groups_per_chunk;
+                const int in_chunk = min(ep.groups_per_chunk, n_groups - k * ep.groups_per_chunk);
+                if (atomicAdd(ep.chunk_done + k, 1u) == (uint32_t)in_chunk - 1u) {
+                    __threadfence_system();
+                    *reinterpret_cast<volatile uint32_t*>(ep.host_flags + k) = ep.epoch;
+                }
+            }
+        }
         if (kCount) {
             unsigned long long cm = 0ull, cp = 0ull;
 #pragma unroll
@@ -730,7 +763,8 @@ size_t walk_stack_entries(int64_t grid_blocks) {
 template <int H, int T>
 static void launch_ht(const Layout& L, const WalkParams& q, const float4* pos, const WalkNode* wn,
                       const WalkGroup* groups, int n_groups, float4* acc, uint32_t* queue, uint32_t* status,
-                      unsigned long long* counts, int2* gstack, int cap, unsigned g, cudaStream_t st) {
+                      unsigned long long* counts, int2* gstack, int cap, unsigned g, cudaStream_t st,
+                      const WalkEpilogue& ep) {
     using Entry = typename EntryOf<T>::type;
     Entry* gs = reinterpret_cast<Entry*>(gstack);
     const size_t sm = smem_bytes<H, T>();
@@ -738,27 +772,28 @@ static void launch_ht(const Layout& L, const WalkParams& q, const float4* pos, c
         if (q.with_potential) {
             configure<H, T, true, true>();
             walk_kernel<H, T, true, true><<<g, kWalkThreads, sm, st>>>(L, q, pos, wn, groups, n_groups, acc, queue,
-                                                                       status, counts, gs, cap);
+                                                                       status, counts, gs, cap, ep);
         } else {
             configure<H, T, false, true>();
             walk_kernel<H, T, false, true><<<g, kWalkThreads, sm, st>>>(L, q, pos, wn, groups, n_groups, acc, queue,
-                                                                        status, counts, gs, cap);
+                                                                        status, counts, gs, cap, ep);
         }
     } else if (q.with_potential) {
         configure<H, T, true, false>();
         walk_kernel<H, T, true, false><<<g, kWalkThreads, sm, st>>>(L, q, pos, wn, groups, n_groups, acc, queue,
-                                                                    status, nullptr, gs, cap);
+                                                                    status, nullptr, gs, cap, ep);
     } else {
         configure<H, T, false, false>();
         walk_kernel<H, T, false, false><<<g, kWalkThreads, sm, st>>>(L, q, pos, wn, groups, n_groups, acc, queue,
-                                                                     status, nullptr, gs, cap);
+                                                                     status, nullptr, gs, cap, ep);
     }
 }
 
 void launch_walk(const Layout& L, const WalkParams& wp, const float4* pos,
                  const WalkNode* wn, const WalkGroup* groups, int n_groups, int targets_per_lane, float4* acc,
                  uint32_t* queue, uint32_t* status, int blocks_per_sm, int sm_count,
-                 unsigned long long* counts, int2* gstack, size_t gstack_entries, cudaStream_t st) {
+                 unsigned long long* counts, int2* gstack, size_t gstack_entries, cudaStream_t st,
+                 const WalkEpilogue& ep) {
     if (n_groups <= 0) return;
     WalkParams q = wp;
     if (q.batch < 1) q.batch = 1;
@@ -783,13 +818,13 @@ void launch_walk(const Layout& L, const WalkParams& wp, const float4* pos,
     const int cap = (int)(std::min<size_t>(units, (size_t)1 << 24) / (size_t)T);
     if (T == 2) {
         if (q.batch > 32)
-            launch_ht<2, 2>(L, q, pos, wn, groups, n_groups, acc, queue, status, counts, gstack, cap, g, st);
+            launch_ht<2, 2>(L, q, pos, wn, groups, n_groups, acc, queue, status, counts, gstack, cap, g, st, ep);
         else
-            launch_ht<1, 2>(L, q, pos, wn, groups, n_groups, acc, queue, status, counts, gstack, cap, g, st);
+            launch_ht<1, 2>(L, q, pos, wn, groups, n_groups, acc, queue, status, counts, gstack, cap, g, st, ep);
     } else if (q.batch > 32) {
-        launch_ht<2, 1>(L, q, pos, wn, groups, n_groups, acc, queue, status, counts, gstack, cap, g, st);
+        launch_ht<2, 1>(L, q, pos, wn, groups, n_groups, acc, queue, status, counts, gstack, cap, g, st, ep);
     } else {
-        launch_ht<1, 1>(L, q, pos, wn, groups, n_groups, acc, queue, status, counts, gstack, cap, g, st);
+        launch_ht<1, 1>(L, q, pos, wn, groups, n_groups, acc, queue, status, counts, gstack, cap, g, st, ep);
     }
 }
 

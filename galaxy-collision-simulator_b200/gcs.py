@@ -294,6 +294,10 @@ class Context:
         self.check(self.L.gcs_step(self._h, C.byref(p)))
 
     def step_host(self, p: Params, out: np.ndarray) -> None:
+        """One step; the stepped Stars (sorted order) land in `out`, copied
+        while the walk runs."""
+        if out.dtype != STAR_DTYPE or len(out) < self.n or not out.flags.c_contiguous:
+            raise ValueError("step_host needs a contiguous Star array of at least n records")
         self.check(self.L.gcs_step_host(self._h, C.byref(p), _ptr(out)))
 
     def compute_accels(self, p: Params) -> None:

@@ -158,9 +158,15 @@ int gcs_step(gcs_ctx* ctx, const gcs_params* p);
 int gcs_set_graphs(gcs_ctx* ctx, int32_t enable);
 /* How many times the step graphs have been captured on this context. */
 int32_t gcs_graph_builds(const gcs_ctx* ctx);
-/* One step, then pack every particle as Star into `host` (pinned for an
- * asynchronous-capable copy) and synchronise: the reference's
- * cuda_physics_step with use_interop=false (cuda_engine.cu:379-451). */
+/* One step with every particle's stepped Star (sorted order) written to
+ * `host`, synchronised on return: the reference's cuda_physics_step with
+ * use_interop=false (cuda_engine.cu:379-451).  Without a step range the copy
+ * overlaps the walk: the walk's epilogue applies the kick/drift and writes
+ * the Star records group by group, and each finished chunk of groups (up to
+ * 32 per step) is copied while later groups are still being walked; `host`
+ * should be pinned for the copies to run asynchronously.  The Stars and the
+ * device state are the same bits as gcs_run_stages(bounds..integrate)
+ * followed by gcs_download_stars. */
 int gcs_step_host(gcs_ctx* ctx, const gcs_params* p, Star* host);
 /* Accelerations at the current positions (bounds..walk, no kick/drift).
  * Afterwards the particle arrays are in this step's Morton order and the
