@@ -331,6 +331,72 @@ def ref_gpu_rate(stars, steps=3):
                     "device time, same GPU"}
 
 
+def dropin_rate(gcs, torch, stars, p, steps=5):
+    """The reference's engine API on both sides: cuda_physics_step(host Stars,
+    ...) called through the C++ symbol of this library (cuda_engine.h) and of
+    the reference's own engine (oracle/_ref), same scenario, caller bounds,
+    theta 0.5, one pinned Star array; wall time per call, the output copy
+    included (the reference copies after the step, this library while the
+    walk runs).  Leaf size: the autotuned one here, 1 in the reference."""
+    import ctypes as C  # noqa: PLC0415
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle  # noqa: PLC0415
+    if oracle.ref_lib("ref_cuda") is None:
+        return None
+    n = len(stars)
+    x = np.stack([stars["x"], stars["y"], stars["z"]])
+    lo, hi = float(x.min()), float(x.max())
+    pad = 0.05 * (hi - lo)
+    lo, hi = lo - pad, hi + pad
+    host = torch.empty(n * 32, dtype=torch.uint8, pin_memory=True)
+    hv = host.numpy().view(gcs.STAR_DTYPE)
+    L = gcs.lib()
+    init = L._Z9cuda_initi
+    init.restype, init.argtypes = C.c_bool, [C.c_int]
+    cleanup = L._Z12cuda_cleanupv
+    cleanup.restype, cleanup.argtypes = None, []
+    upload = L._Z25cuda_upload_initial_starsPK4Stari
+    upload.restype, upload.argtypes = None, [C.c_void_p, C.c_int]
+    step = L._Z17cuda_physics_stepP4Starifffffb
+    step.restype = C.c_float
+    step.argtypes = [C.c_void_p, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_bool]
+    q = make_params(gcs, p.leaf_size, p.walk_batch)
+    q.bounds_mode = gcs.BOUNDS_CALLER
+    q.walk_blocks_per_sm = p.walk_blocks_per_sm
+    out = {"workload": "%d particles, cuda_physics_step with a pinned host Star array, caller bounds, "
+                       "theta %.1f, %d calls after 2 warm-up calls, median wall time" % (n, THETA, steps)}
+    ms = []
+    if not init(n):
+        return None
+    try:
+        L.gcs_dropin_set_params(C.byref(q))
+        upload(stars.ctypes.data, n)
+        for k in range(steps + 2):
+            t0 = time.perf_counter()
+            step(hv.ctypes.data, n, 1.0, EPS * EPS, DT, lo, hi, False)
+            if k >= 2:
+                ms.append((time.perf_counter() - t0) * 1e3)
+    finally:
+        cleanup()
+    t = statistics.median(ms)
+    out["gcs"] = {"value": n / (t / 1e3), "unit": "particle-steps/s", "ms_per_call": t, "leaf_size": q.leaf_size}
+    ref = oracle.RefCuda(n)
+    ms = []
+    try:
+        ref.set_theta(THETA)
+        ref.upload(stars)
+        for k in range(steps + 2):
+            t0 = time.perf_counter()
+            ref.step(hv, 1.0, EPS * EPS, DT, lo, hi)
+            if k >= 2:
+                ms.append((time.perf_counter() - t0) * 1e3)
+    finally:
+        ref.close()
+    t = statistics.median(ms)
+    out["reference"] = {"value": n / (t / 1e3), "unit": "particle-steps/s", "ms_per_call": t, "leaf_size": 1}
+    return out
+
+
 def accuracy(gcs, ctx, p, stars, n_sub=65536, seed=0):
     """Median / p99 relative force error against an FP64 direct sum (GPU,
     excluding only i == j) on a seeded subset of targets, for this engine
@@ -869,6 +935,7 @@ def main():
             line["accuracy"] = accuracy(gcs, ctx, p, stars)
         if not args.no_ref_gpu:
             line["ref_gpu"] = ref_gpu_rate(stars)
+            line["dropin"] = dropin_rate(gcs, torch, stars, p)
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_reference_rate(stars, args.cpu_seconds)
         if not args.no_render:
