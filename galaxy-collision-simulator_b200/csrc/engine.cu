@@ -1289,6 +1289,22 @@ int gcs_render_stars(const Star* stars, int64_t n, const gcs_camera* cam, int32_
     return cudaGetLastError() == cudaSuccess ? GCS_OK : GCS_ERR_CUDA;
 }
 
+int gcs_render_playback(const PlaybackStar* frame, int64_t n, const gcs_camera* cam, int32_t width, int32_t height,
+                        uint64_t* accum, uint8_t* rgba, void* stream) {
+    if (n < 0 || (n > 0 && !frame) || !cam || !accum || width < 1 || height < 1) return GCS_ERR_ARG;
+    const int64_t pixels = (int64_t)width * height;
+    if (pixels > ((int64_t)1 << 28)) return GCS_ERR_ARG;
+    if ((reinterpret_cast<uintptr_t>(accum) & 7u) || (reinterpret_cast<uintptr_t>(rgba) & 3u) ||
+        (reinterpret_cast<uintptr_t>(frame) & 15u))
+        return GCS_ERR_ARG;
+    float view[16], proj[16];
+    if (gcs_camera_matrices(cam, width, height, view, proj)) return GCS_ERR_ARG;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    launch_splat_playback(frame, n, view, proj, width, height, reinterpret_cast<unsigned long long*>(accum), st);
+    if (rgba) launch_resolve(reinterpret_cast<const unsigned long long*>(accum), pixels, rgba, st);
+    return cudaGetLastError() == cudaSuccess ? GCS_OK : GCS_ERR_CUDA;
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------

@@ -187,6 +187,8 @@ void launch_splat_posvel(const float4* pos, const float4* vel, int64_t n, const 
                          int width, int height, unsigned long long* acc, cudaStream_t st);
 void launch_splat_stars(const Star* stars, int64_t n, const float* view, const float* proj, int width, int height,
                         unsigned long long* acc, cudaStream_t st);
+void launch_splat_playback(const PlaybackStar* recs, int64_t n, const float* view, const float* proj, int width,
+                           int height, unsigned long long* acc, cudaStream_t st);
 void launch_resolve(const unsigned long long* acc, int64_t pixels, uint8_t* rgba, cudaStream_t st);
 
 void launch_direct_fp64(const float4* pos, int64_t seg_first, int64_t seg_n, const int64_t* targets,

@@ -60,6 +60,20 @@ struct StarSource {
     }
 };
 
+// Position and packed type|r|g|b from PlaybackStar records (bytes 12..15 are
+// r, g, b, type: the same word rotated by one byte).
+struct PlaybackSource {
+    const PlaybackStar* recs;
+    __device__ __forceinline__ void get(int64_t i, float& x, float& y, float& z, uint32_t& tcol) const {
+        const float4 a = __ldg(reinterpret_cast<const float4*>(recs + i));
+        x = a.x;
+        y = a.y;
+        z = a.z;
+        const uint32_t w = __float_as_uint(a.w);
+        tcol = (w << 8) | (w >> 24);
+    }
+};
+
 // Row r of a 4x4 row-major matrix times (x, y, z, 1).
 __device__ __forceinline__ float row_dot(const float* m, int r, float x, float y, float z) {
     return __fmaf_rn(m[4 * r + 0], x, __fmaf_rn(m[4 * r + 1], y, __fmaf_rn(m[4 * r + 2], z, m[4 * r + 3])));
@@ -179,6 +193,12 @@ void launch_splat_stars(const Star* stars, int64_t n, const float* view, const f
                         unsigned long long* acc, cudaStream_t st) {
     if (n <= 0) return;
     splat_kernel<<<splat_grid(n), 256, 0, st>>>(StarSource{stars}, n, mats_of(view, proj, width, height), acc);
+}
+
+void launch_splat_playback(const PlaybackStar* recs, int64_t n, const float* view, const float* proj, int width,
+                           int height, unsigned long long* acc, cudaStream_t st) {
+    if (n <= 0) return;
+    splat_kernel<<<splat_grid(n), 256, 0, st>>>(PlaybackSource{recs}, n, mats_of(view, proj, width, height), acc);
 }
 
 void launch_resolve(const unsigned long long* acc, int64_t pixels, uint8_t* rgba, cudaStream_t st) {

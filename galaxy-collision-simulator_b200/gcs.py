@@ -138,6 +138,16 @@ def lib() -> C.CDLL:
         "gcs_camera_matrices": (C.c_int, [C.POINTER(Camera), i32, i32, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
         "gcs_render_frame": (C.c_int, [P, C.POINTER(Camera), i32, i32, i32, P, i32]),
         "gcs_render_stars": (C.c_int, [P, i64, C.POINTER(Camera), i32, i32, P, P, P]),
+        "gcs_render_playback": (C.c_int, [P, i64, C.POINTER(Camera), i32, i32, P, P, P]),
+        "gcs_playback_open": (C.c_int, [C.c_char_p, i64, i64, C.POINTER(P)]),
+        "gcs_playback_frames": (i64, [P]),
+        "gcs_playback_particles": (i64, [P]),
+        "gcs_playback_position": (i64, [P]),
+        "gcs_playback_next": (C.c_int, [P, P]),
+        "gcs_playback_prev": (C.c_int, [P, P]),
+        "gcs_playback_seek": (C.c_int, [P, i64]),
+        "gcs_playback_centre": (C.c_int, [P, i64, P]),
+        "gcs_playback_close": (None, [P]),
         "gcs_server_create": (C.c_int, [C.POINTER(P), i32, i64, i32, C.c_double, C.POINTER(Params)]),
         "gcs_server_destroy": (None, [P]),
         "gcs_server_context": (P, [P]),
@@ -539,6 +549,67 @@ def read_playback(path: str, n: int) -> np.ndarray:
     if len(raw) % n:
         raise GcsError("%s holds %d records, not a whole number of %d-star frames" % (path, len(raw), n))
     return raw.reshape(-1, n)
+
+
+class Playback:
+    """A simulation.bin file read back frame by frame (gcs_playback_*): the
+    reference's Playback mode without its window.  particles > 0 gives the
+    records per frame; particles = 0 infers it from frames_hint frames, as
+    the reference does with 2000."""
+
+    def __init__(self, path: str, particles: int = 0, frames_hint: int = 2000):
+        self.L = lib()
+        self._h = C.c_void_p()
+        rc = self.L.gcs_playback_open(os.fsencode(path), particles, frames_hint, C.byref(self._h))
+        if rc != OK:
+            raise GcsError("gcs_playback_open(%s): %s" % (path, self.L.gcs_status_string(rc).decode()))
+        self.frames = int(self.L.gcs_playback_frames(self._h))
+        self.particles = int(self.L.gcs_playback_particles(self._h))
+
+    def close(self) -> None:
+        if self._h:
+            self.L.gcs_playback_close(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def position(self) -> int:
+        return int(self.L.gcs_playback_position(self._h))
+
+    def _read(self, fn) -> np.ndarray:
+        out = np.zeros(self.particles, dtype=PLAYBACK_DTYPE)
+        rc = fn(self._h, _ptr(out))
+        if rc != OK:
+            raise GcsError("playback read: %s" % self.L.gcs_status_string(rc).decode())
+        return out
+
+    def next(self) -> np.ndarray:
+        return self._read(self.L.gcs_playback_next)
+
+    def prev(self) -> np.ndarray:
+        return self._read(self.L.gcs_playback_prev)
+
+    def seek(self, frame: int) -> None:
+        _check(self.L.gcs_playback_seek(self._h, frame), None)
+
+
+def playback_centre(frame: np.ndarray) -> np.ndarray:
+    """The reference's per-frame camera target: FP64 mean position as float."""
+    frame = np.ascontiguousarray(frame, dtype=PLAYBACK_DTYPE)
+    out = np.zeros(3, np.float32)
+    _check(lib().gcs_playback_centre(_ptr(frame), len(frame), _ptr(out)), None)
+    return out
 
 
 def camera_reference() -> Camera:

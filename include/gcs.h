@@ -331,6 +331,34 @@ int64_t gcs_context_bytes(int64_t capacity, int32_t max_segments, int32_t device
 int gcs_bake(gcs_ctx* ctx, const gcs_params* p, int32_t frames, const char* path, int32_t append,
              double* seconds);
 
+/* ---- playback ----------------------------------------------------------------
+ * Reading a simulation.bin file back frame by frame: the reference's Playback
+ * mode (main.cpp:299-453) without its window.  Host only; no GPU is needed.
+ * particles > 0: records per frame; the file must hold a whole number of
+ * frames of that size.  particles = 0: the reference's inference, particles =
+ * file size / frames_hint / 16 (the reference hard-codes 2000 frames,
+ * main.cpp:309), and only whole frames are kept.  Errors: GCS_ERR_ARG (no
+ * such file, an empty file, a size that is not a whole number of frames,
+ * bad arguments), GCS_ERR_NOMEM. */
+typedef struct gcs_playback gcs_playback;
+int gcs_playback_open(const char* path, int64_t particles, int64_t frames_hint, gcs_playback** out);
+int64_t gcs_playback_frames(const gcs_playback* pb);
+int64_t gcs_playback_particles(const gcs_playback* pb);
+/* The frame the next gcs_playback_next returns. */
+int64_t gcs_playback_position(const gcs_playback* pb);
+/* Read the next frame into `host` (particles records); after the last frame
+ * playback loops to the first (main.cpp:413-419). */
+int gcs_playback_next(gcs_playback* pb, PlaybackStar* host);
+/* Step back: the frame before the one last read, or the last frame when that
+ * is before the first (main.cpp:397-410); reading goes on forward from it. */
+int gcs_playback_prev(gcs_playback* pb, PlaybackStar* host);
+/* Move so that the next read returns `frame` (taken modulo the frame count). */
+int gcs_playback_seek(gcs_playback* pb, int64_t frame);
+/* The camera target of a frame: the mean position in FP64, rounded to float
+ * (main.cpp:435-441). */
+int gcs_playback_centre(const PlaybackStar* frame, int64_t n, float centre[3]);
+void gcs_playback_close(gcs_playback* pb);
+
 /* ---- headless point-splat renderer ------------------------------------------
  * The reference draws every Star as one GL point (renderer.cpp:97-148,
  * vertex attributes 226-233): the
@@ -380,6 +408,13 @@ int gcs_render_frame(gcs_ctx* ctx, const gcs_camera* cam, int32_t segment, int32
  * 16-byte aligned, accum 8-byte and rgba 4-byte aligned. */
 int gcs_render_stars(const Star* stars, int64_t n, const gcs_camera* cam, int32_t width,
                      int32_t height, uint64_t* accum, uint8_t* rgba, void* stream);
+/* As gcs_render_stars for n device PlaybackStar records (a simulation.bin
+ * frame copied to the device): the reference's Playback mode draws a frame's
+ * records as Stars with the same position, colour and type (main.cpp:423-433),
+ * so a frame renders exactly as the Stars it was written from.  frame must
+ * be 16-byte aligned. */
+int gcs_render_playback(const PlaybackStar* frame, int64_t n, const gcs_camera* cam, int32_t width,
+                        int32_t height, uint64_t* accum, uint8_t* rgba, void* stream);
 
 /* ---- serving ---------------------------------------------------------------
  * Continuous batching of independent collision scenarios on one device (no
