@@ -17,6 +17,8 @@
 #include <thread>
 #include <vector>
 
+#include <cuda.h>  // driver API types for the pointer-range query (entry point fetched at run time)
+
 #include "gcs_internal.h"
 
 using namespace gcs;
@@ -852,6 +854,41 @@ int gcs_set_graphs(gcs_ctx* c, int32_t enable) {
 
 int32_t gcs_graph_builds(const gcs_ctx* c) { return c ? c->graph_builds : 0; }
 
+// The device address of the `bytes` at host pointer p when all of them lie in
+// one pinned, device-mapped host allocation (cudaMallocHost, cudaHostAlloc,
+// cudaHostRegister with UVA), 16-byte aligned; nullptr otherwise.  The range
+// comes from the driver (cuPointerGetAttribute, RANGE_START_ADDR / _SIZE),
+// fetched through the runtime's entry-point query, so the library does not
+// link the driver library.
+static void* mapped_host_range(const void* p, size_t bytes) {
+    using GetAttr = CUresult (*)(void*, CUpointer_attribute, CUdeviceptr);
+    static GetAttr get_attr = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuPointerGetAttribute", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_attr = reinterpret_cast<GetAttr>(f);
+        cudaGetLastError();
+    });
+    if (!p || !get_attr) return nullptr;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();  // not memory the runtime knows: pageable
+        return nullptr;
+    }
+    if (a.type != cudaMemoryTypeHost || !a.devicePointer) return nullptr;
+    const CUdeviceptr d = reinterpret_cast<CUdeviceptr>(a.devicePointer);
+    CUdeviceptr start = 0;
+    size_t size = 0;
+    if (get_attr(&start, CU_POINTER_ATTRIBUTE_RANGE_START_ADDR, d) != CUDA_SUCCESS ||
+        get_attr(&size, CU_POINTER_ATTRIBUTE_RANGE_SIZE, d) != CUDA_SUCCESS)
+        return nullptr;
+    if (d < start || d - start > size || bytes > size - (d - start) || (d & 15u)) return nullptr;
+    return a.devicePointer;
+}
+
 // Resources of the overlapped host step, created at its first use.
 static int ensure_star_pipeline(gcs_ctx* c) {
     if (!c->star_stream) GCS_CUDA(c, cudaStreamCreateWithFlags(&c->star_stream, cudaStreamNonBlocking));
@@ -869,20 +906,50 @@ static int ensure_star_pipeline(gcs_ctx* c) {
     return GCS_OK;
 }
 
-// One step whose Stars land in `host`, with the copy overlapped with the
+// One step whose Stars land in `host`, with the transfer overlapped with the
 // walk: the walk's epilogue applies the kick/drift out of place and writes
-// each group's Star records; the host copies every chunk of groups (up to
-// kMaxStarChunks per step) as soon as its flag arrives.  The result is the
+// each group's Star records, straight into `host` when it is pinned and
+// device-mapped, else into device staging, from which the host copies every
+// chunk of groups as soon as its flag arrives.  Groups handed out before the work queue runs dry go
+// in up to kMaxStarHeadChunks large chunks; the last groups (twice the
+// walk's resident warps, one group each) are all in flight at the end and
+// finish together, so they go in up to kMaxStarTailChunks small chunks whose
+// completions, and copies, spread over the walk's last phase.  The result is the
 // same bits as the plain stage sequence followed by gcs_download_stars.  A
 // step range (one slice of the scenario) takes that plain sequence.
 static int step_host_overlapped(gcs_ctx* c, const gcs_params* p, Star* host) {
     int rc = run_stages(c, p, GCS_STAGE_BOUNDS, GCS_STAGE_AGGREGATE);
     if (rc) return rc;
+    // A pinned, device-mapped host array: the epilogue writes each group's
+    // Stars straight into it over PCIe while the walk goes on (no copies, no
+    // flags); the stream's completion makes them visible to the host.
+    void* direct = mapped_host_range(host, sizeof(Star) * (size_t)c->n);
+    if (direct) {
+        WalkEpilogue ep;
+        ep.vel_in = c->vel[c->cur];
+        ep.pos_out = c->pos[c->cur ^ 1];
+        ep.vel_out = c->vel[c->cur ^ 1];
+        ep.stars = reinterpret_cast<float4*>(direct);
+        ep.dt = p->dt;
+        ep.recolor = p->recolor;
+        rc = walk_stage(c, p, ep);
+        if (rc) return rc;
+        c->cur ^= 1;  // the epilogue wrote the stepped state into the other arrays
+        GCS_CUDA(c, cudaStreamSynchronize(c->stream));
+        return GCS_OK;
+    }
     rc = ensure_star_pipeline(c);
     if (rc) return rc;
     const int ng = c->n_groups;
-    const int gpc = (ng + kMaxStarChunks - 1) / kMaxStarChunks;
-    const int chunks = (ng + gpc - 1) / gpc;
+    const int64_t resident = walk_grid_blocks(ng, p->walk_blocks_per_sm, c->sm_count, p->with_potential) *
+                             (int64_t)kWalkBlockWarps;
+    const int tail_groups = (int)std::min<int64_t>(ng, 2 * resident);
+    const int head_groups = ng - tail_groups;
+    const int hpc = head_groups > 0 ? (head_groups + kMaxStarHeadChunks - 1) / kMaxStarHeadChunks : 1;
+    const int head_chunks = head_groups > 0 ? (head_groups + hpc - 1) / hpc : 0;
+    const int tpc = (tail_groups + kMaxStarTailChunks - 1) / kMaxStarTailChunks;
+    const int tail_chunks = (tail_groups + tpc - 1) / tpc;
+    const int chunks = head_chunks + tail_chunks;
     if (++c->star_epoch == 0) c->star_epoch = 1;
     const uint32_t epoch = c->star_epoch;
     GCS_CUDA(c, cudaMemsetAsync(c->star_chunk_done, 0, sizeof(uint32_t) * (size_t)chunks, c->stream));
@@ -893,7 +960,10 @@ static int step_host_overlapped(gcs_ctx* c, const gcs_params* p, Star* host) {
     ep.stars = reinterpret_cast<float4*>(c->staging);
     ep.dt = p->dt;
     ep.recolor = p->recolor;
-    ep.groups_per_chunk = gpc;
+    ep.head_groups = head_groups;
+    ep.head_per_chunk = hpc;
+    ep.head_chunks = head_chunks;
+    ep.tail_per_chunk = tpc;
     ep.chunk_done = c->star_chunk_done;
     ep.host_flags = c->star_flags_dev;
     ep.epoch = epoch;
@@ -905,8 +975,11 @@ static int step_host_overlapped(gcs_ctx* c, const gcs_params* p, Star* host) {
     // what is left (a chunk that was never signalled is reported).
     bool missing = false;
     for (int k = 0; k < chunks && !rc; ++k) {
-        const int64_t first = c->h_group_start[(size_t)k * gpc];
-        const int64_t end = (int64_t)(k + 1) * gpc < ng ? c->h_group_start[(size_t)(k + 1) * gpc] : c->n;
+        const int g0 = k < head_chunks ? k * hpc : head_groups + (k - head_chunks) * tpc;
+        const int g1 = k < head_chunks ? std::min((k + 1) * hpc, head_groups)
+                                       : std::min(head_groups + (k - head_chunks + 1) * tpc, ng);
+        const int64_t first = c->h_group_start[(size_t)g0];
+        const int64_t end = g1 < ng ? c->h_group_start[(size_t)g1] : c->n;
         for (uint32_t polls = 1;; ++polls) {
             if (__atomic_load_n(c->star_flags + k, __ATOMIC_ACQUIRE) == epoch) break;
             if ((polls & 63u) == 0u) {

@@ -140,12 +140,17 @@ constexpr int kWalkMaxBatch = 64;  // nodes popped per walk round
 // Optional epilogue of the walk: each warp, once its group's accelerations
 // are written, applies the kick/drift to the group's particles out of place
 // (pos/vel_in -> pos_out/vel_out, so the walk's other warps keep reading the
-// step's positions) and writes their Star records.  Groups are counted per
-// chunk of `groups_per_chunk` consecutive groups; the warp that completes a
-// chunk stores `epoch` into host_flags[chunk] (mapped host memory, after a
-// system-scope fence), so the host can copy that chunk's Stars while the
-// walk continues.  vel_in == nullptr: no epilogue.  chunk_done must be zero
-// at launch.
+// step's positions) and writes their Star records.  Groups are counted in
+// chunks of consecutive groups: `head_chunks` chunks of `head_per_chunk`
+// over the first `head_groups` groups, then chunks of `tail_per_chunk` over
+// the rest (the groups still in flight when the work queue runs dry, which
+// finish together at the end of the walk: small chunks there spread their
+// completions out).  The warp that completes a chunk stores `epoch` into
+// host_flags[chunk] (mapped host memory, after a system-scope fence), so the
+// host can copy that chunk's Stars while the walk continues; with
+// host_flags == nullptr nothing is counted (the records go straight to
+// pinned host memory).  vel_in == nullptr: no epilogue.  chunk_done must be
+// zero at launch.
 struct WalkEpilogue {
     const float4* vel_in = nullptr;
     float4* pos_out = nullptr;
@@ -153,12 +158,18 @@ struct WalkEpilogue {
     float4* stars = nullptr;  // Star records as float4 pairs
     float dt = 0.0f;
     int32_t recolor = 0;
-    int32_t groups_per_chunk = 1;
+    int32_t head_groups = 0;
+    int32_t head_per_chunk = 1;
+    int32_t head_chunks = 0;
+    int32_t tail_per_chunk = 1;
     uint32_t* chunk_done = nullptr;
     uint32_t* host_flags = nullptr;
     uint32_t epoch = 0;
 };
-constexpr int kMaxStarChunks = 32;
+constexpr int kMaxStarHeadChunks = 16;
+constexpr int kMaxStarTailChunks = 48;
+constexpr int kMaxStarChunks = kMaxStarHeadChunks + kMaxStarTailChunks;
+constexpr int kWalkBlockWarps = 8;  // warps per walk block
 
 void launch_walk(const Layout& L, const WalkParams& wp, const float4* pos,
                  const WalkNode* wn, const WalkGroup* groups, int n_groups, int targets_per_lane,

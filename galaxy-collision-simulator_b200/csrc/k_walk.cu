@@ -54,9 +54,13 @@
 // With an epilogue (WalkEpilogue), a warp that has written its group's
 // accelerations also applies the step's kick/drift to those particles, out of
 // place, and writes their Star records; the warp that completes a chunk of
-// groups raises that chunk's flag in mapped host memory.  The host copies
+// groups raises that chunk's flag in mapped host memory (chunks are large
+// over the groups handed out early and small over the last ones, which are
+// all in flight together at the end).  The host copies
 // finished chunks to its Star array while the walk is still running (the
-// reference copies all Stars after the step, cuda_engine.cu:442-448).
+// reference copies all Stars after the step, cuda_engine.cu:442-448).  When
+// the Star array is pinned host memory mapped into the device, the records
+// go straight into it and no chunk is counted (host_flags == nullptr).
 #include <algorithm>
 
 #include "gcs_internal.h"
@@ -66,7 +70,7 @@ namespace gcs {
 
 namespace {
 
-constexpr int kWalkWarps = 8;
+constexpr int kWalkWarps = kWalkBlockWarps;
 constexpr int kWalkThreads = kWalkWarps * 32;
 constexpr int kSpillCount = 128;  // entries moved per spill / refill
 constexpr int kSrcCap = 64;
@@ -648,15 +652,22 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                 store_star(ep.stars, i, p, v);
             }
         }
-        if (ep.vel_in) {
+        if (ep.vel_in && ep.host_flags) {
             // count the group in its chunk; the warp that completes the chunk
             // tells the host (every warp fences before counting, so a chunk
             // seen complete has all of its records written)
             __syncwarp();
             if (lane == 0) {
                 __threadfence();
-                const int k = g / ep.groups_per_chunk;
-                const int in_chunk = min(ep.groups_per_chunk, n_groups - k * ep.groups_per_chunk);
+                int k, in_chunk;
+                if (g < ep.head_groups) {
+                    k = g / ep.head_per_chunk;
+                    in_chunk = min(ep.head_per_chunk, ep.head_groups - k * ep.head_per_chunk);
+                } else {
+                    const int j = (g - ep.head_groups) / ep.tail_per_chunk;
+                    k = ep.head_chunks + j;
+                    in_chunk = min(ep.tail_per_chunk, n_groups - ep.head_groups - j * ep.tail_per_chunk);
+                }
                 if (atomicAdd(ep.chunk_done + k, 1u) == (uint32_t)in_chunk - 1u) {
                     __threadfence_system();
                     *reinterpret_cast<volatile uint32_t*>(ep.host_flags + k) = ep.epoch;

@@ -160,13 +160,17 @@ int gcs_set_graphs(gcs_ctx* ctx, int32_t enable);
 int32_t gcs_graph_builds(const gcs_ctx* ctx);
 /* One step with every particle's stepped Star (sorted order) written to
  * `host`, synchronised on return: the reference's cuda_physics_step with
- * use_interop=false (cuda_engine.cu:379-451).  Without a step range the copy
- * overlaps the walk: the walk's epilogue applies the kick/drift and writes
- * the Star records group by group, and each finished chunk of groups (up to
- * 32 per step) is copied while later groups are still being walked; `host`
- * should be pinned for the copies to run asynchronously.  The Stars and the
- * device state are the same bits as gcs_run_stages(bounds..integrate)
- * followed by gcs_download_stars. */
+ * use_interop=false (cuda_engine.cu:379-451).  Without a step range the
+ * transfer overlaps the walk: the walk's epilogue applies the kick/drift and
+ * writes the Star records group by group.  When `host` is pinned host memory
+ * mapped into the device (cudaMallocHost, cudaHostAlloc, registered memory;
+ * all n records inside one allocation, 16-byte aligned), the records are
+ * written straight into it over PCIe; otherwise each finished chunk of groups
+ * is copied from device staging while later groups are still being walked
+ * (up to 64 chunks a step: large ones over the groups handed out early,
+ * small ones over the last groups, which finish together at the end).  The
+ * Stars and the device state are the same bits as
+ * gcs_run_stages(bounds..integrate) followed by gcs_download_stars. */
 int gcs_step_host(gcs_ctx* ctx, const gcs_params* p, Star* host);
 /* Accelerations at the current positions (bounds..walk, no kick/drift).
  * Afterwards the particle arrays are in this step's Morton order and the

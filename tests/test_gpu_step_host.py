@@ -1,8 +1,9 @@
-"""The host step with the Star copy overlapped with the walk (gcs_step_host).
+"""The host step with the Star transfer overlapped with the walk (gcs_step_host).
 
 The walk's epilogue applies the kick/drift out of place and writes the Star
-records; the host copies each finished chunk of walk groups while the walk
-runs.  The Stars it returns, and the state it leaves on the device, must be
+records: straight into the caller's array when it is pinned, device-mapped
+host memory (16-byte aligned), else into device staging, from which the host
+copies each finished chunk of walk groups while the walk runs.  The Stars it returns, and the state it leaves on the device, must be
 the same bits as the plain stage sequence (bounds .. integrate) followed by
 gcs_download_stars, step after step: for one and several segments, both
 group widths, ragged sizes (1, 2, 33 particles; groups that do not fill a
@@ -23,14 +24,26 @@ def _params(gcs, leaf=4, batch=64):
                                 bounds_mode=gcs.BOUNDS_DEVICE, com_fp64=1)
 
 
-def _pair(gcs, stars, counts, width, p, steps, graphs_every=0):
+def _pinned_stars(gcs, n, byte_offset=0):
+    """A Star array in pinned host memory (optionally starting byte_offset
+    bytes into the pinned block)."""
+    import torch
+    block = torch.zeros(n * 32 + 64, dtype=torch.uint8, pin_memory=True)
+    arr = block.numpy()[byte_offset:byte_offset + n * 32].view(gcs.STAR_DTYPE)
+    return block, arr
+
+
+def _pair(gcs, stars, counts, width, p, steps, graphs_every=0, pinned=False, byte_offset=0):
     n = len(stars)
     with gcs.Context(n, max_segments=len(counts)) as a, gcs.Context(n, max_segments=len(counts)) as b:
         for ctx in (a, b):
             ctx.set_segments(counts)
             ctx.set_group_width(width)
             ctx.upload(stars)
-        out = np.zeros(n, dtype=gcs.STAR_DTYPE)
+        if pinned:
+            keep, out = _pinned_stars(gcs, n, byte_offset)
+        else:
+            out = np.zeros(n, dtype=gcs.STAR_DTYPE)
         for k in range(steps):
             if graphs_every and k % graphs_every == graphs_every - 1:
                 # a plain (graph-captured) step on the overlapped context
@@ -56,15 +69,34 @@ def _pair(gcs, stars, counts, width, p, steps, graphs_every=0):
 
 
 @pytest.mark.parametrize("width", [32, 64])
-def test_overlapped_host_step_equals_plain_step(gcs_mod, width):
+@pytest.mark.parametrize("pinned", [False, True])
+def test_overlapped_host_step_equals_plain_step(gcs_mod, width, pinned):
     gcs = gcs_mod
     stars = small_collision(3000, 700, 300, seed=17)  # 8,000 particles, 250 or 125 groups
-    _pair(gcs, stars, [len(stars)], width, _params(gcs), steps=4)
+    _pair(gcs, stars, [len(stars)], width, _params(gcs), steps=4, pinned=pinned)
+
+
+@pytest.mark.parametrize("byte_offset", [32, 8])
+def test_pinned_array_inside_a_block(gcs_mod, byte_offset):
+    """A pinned array one Star into its block is written directly; one that
+    starts 8 bytes in (not 16-byte aligned) takes the copy path; both give
+    the same bytes."""
+    gcs = gcs_mod
+    stars = small_collision(3000, 700, 300, seed=25)
+    _pair(gcs, stars, [len(stars)], 32, _params(gcs), steps=2, pinned=True, byte_offset=byte_offset)
 
 
 def test_overlapped_host_step_many_chunks(gcs_mod):
     gcs = gcs_mod
-    stars = small_collision(30000, 7000, 3000, seed=18)  # 80,000 particles: 2,500 groups, 32 chunks
+    stars = small_collision(30000, 7000, 3000, seed=18)  # 80,000 particles: 2,500 groups, 48 chunks
+    _pair(gcs, stars, [len(stars)], 32, _params(gcs), steps=2)
+
+
+def test_overlapped_host_step_head_and_tail_chunks(gcs_mod):
+    """400,000 particles: 12,500 groups, more than twice the walk's resident
+    warps, so both the large head chunks and the small tail chunks are used."""
+    gcs = gcs_mod
+    stars = small_collision(150000, 37500, 12500, seed=24)
     _pair(gcs, stars, [len(stars)], 32, _params(gcs), steps=2)
 
 
@@ -73,13 +105,15 @@ def test_overlapped_host_step_segments(gcs_mod):
     stars = small_collision(3000, 700, 300, seed=19)
     counts = [5000, 33, 1, 2966]
     _pair(gcs, stars, counts, 32, _params(gcs, leaf=8, batch=32), steps=3)
+    _pair(gcs, stars, counts, 32, _params(gcs, leaf=8, batch=32), steps=3, pinned=True)
 
 
 @pytest.mark.parametrize("n", [1, 2, 33, 1000])
-def test_overlapped_host_step_ragged(gcs_mod, n):
+@pytest.mark.parametrize("pinned", [False, True])
+def test_overlapped_host_step_ragged(gcs_mod, n, pinned):
     gcs = gcs_mod
     stars = small_collision(3000, 700, 300, seed=20)[:n].copy()
-    _pair(gcs, stars, [n], 32, _params(gcs), steps=2)
+    _pair(gcs, stars, [n], 32, _params(gcs), steps=2, pinned=pinned)
 
 
 def test_overlapped_host_step_between_graph_steps(gcs_mod):
@@ -126,7 +160,7 @@ def test_dropin_host_step_equals_engine_steps(gcs_mod):
     assert init(n)
     try:
         upload(stars.ctypes.data, n)
-        host = np.zeros(n, dtype=gcs.STAR_DTYPE)
+        keep, host = _pinned_stars(gcs, n)  # the Bake driver's pinned array
         p = gcs.Params()
         L.gcs_params_reference(C.byref(p))
         p.G, p.epsilon_sq, p.dt, p.global_min, p.global_max = 1.0, 10.0, 0.01, lo, hi
