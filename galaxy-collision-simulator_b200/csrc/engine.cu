@@ -1262,6 +1262,15 @@ void gcs_camera_reference(gcs_camera* cam) {
     cam->z_far = 5000.0f;
 }
 
+int gcs_camera_look_at(gcs_camera* cam, const float target[3]) {
+    if (!cam || !target) return GCS_ERR_ARG;
+    const float d[3] = {target[0] - cam->pos[0], target[1] - cam->pos[1], target[2] - cam->pos[2]};
+    const float len = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    if (!(len > 0.0f) || !std::isfinite(len)) return GCS_ERR_ARG;
+    for (int k = 0; k < 3; ++k) cam->front[k] = d[k] * (1.0f / len);
+    return GCS_OK;
+}
+
 // View = lookAt(eye, eye + front, up): rows s, u, -f (s = normalize(f x up),
 // u = s x f, f = normalize(front)) with translations -s.eye, -u.eye, f.eye.
 // Proj = perspective(fovy, aspect, near, far), OpenGL clip depth [-1, 1].

@@ -136,6 +136,7 @@ def lib() -> C.CDLL:
         "gcs_device_array": (P, [P, i32]),
         "gcs_camera_reference": (None, [C.POINTER(Camera)]),
         "gcs_camera_matrices": (C.c_int, [C.POINTER(Camera), i32, i32, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+        "gcs_camera_look_at": (C.c_int, [C.POINTER(Camera), C.POINTER(C.c_float)]),
         "gcs_render_frame": (C.c_int, [P, C.POINTER(Camera), i32, i32, i32, P, i32]),
         "gcs_render_stars": (C.c_int, [P, i64, C.POINTER(Camera), i32, i32, P, P, P]),
         "gcs_render_playback": (C.c_int, [P, i64, C.POINTER(Camera), i32, i32, P, P, P]),
@@ -616,6 +617,15 @@ def camera_reference() -> Camera:
     """The reference's start-up camera (renderer.cpp:9-11, 263)."""
     cam = Camera()
     lib().gcs_camera_reference(C.byref(cam))
+    return cam
+
+
+def camera_look_at(cam: Camera, target) -> Camera:
+    """Point cam at target (front = normalize(target - pos)); returns cam."""
+    t = (C.c_float * 3)(*[float(x) for x in target])
+    rc = lib().gcs_camera_look_at(C.byref(cam), t)
+    if rc != OK:
+        raise GcsError("gcs_camera_look_at: status %d" % rc)
     return cam
 
 

@@ -391,6 +391,12 @@ typedef struct gcs_camera {
 /* The reference's start-up camera: eye (0, 150, 600), front (0, -0.2, -1),
  * up (0, 1, 0), 45 degrees, near 0.1, far 5000. */
 void gcs_camera_reference(gcs_camera* cam);
+/* Point the camera at `target` from where it stands: front = normalize(target -
+ * pos), as the reference does every frame while the camera is locked on the
+ * centre of mass or, in Playback mode, the frame's mean position
+ * (renderer.cpp:255-256; the target from gcs_playback_centre or
+ * cuda_get_center_of_mass).  GCS_ERR_ARG when target is the eye. */
+int gcs_camera_look_at(gcs_camera* cam, const float target[3]);
 /* The 4x4 view and projection matrices (row-major, applied to column
  * vectors) the renderer uses for cam at width x height: glm::lookAt(pos,
  * pos + front, up) and glm::perspective(fovy, width/height, near, far). */

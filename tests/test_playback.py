@@ -143,3 +143,20 @@ def test_render_playback_rejects_bad_arguments(gcs_mod):
     assert L.gcs_render_playback(None, 10, C.byref(cam), 8, 8, acc.ctypes.data, None, None) != gcs.OK
     assert L.gcs_render_playback(acc.ctypes.data, 1, C.byref(cam), 0, 8, acc.ctypes.data, None, None) != gcs.OK
     assert L.gcs_render_playback(acc.ctypes.data + 4, 1, C.byref(cam), 8, 8, acc.ctypes.data, None, None) != gcs.OK
+
+
+def test_camera_locks_on_the_frame_centre(gcs_mod):
+    """renderer.cpp:255-256: front = normalize(target - pos); the view then
+    puts the target on the axis in front of the eye."""
+    gcs = gcs_mod
+    cam = gcs.camera_reference()
+    target = np.array([12.5, -3.0, 40.0], np.float32)
+    gcs.camera_look_at(cam, target)
+    d = target - np.array(cam.pos[:], np.float32)
+    want = d * (np.float32(1.0) / np.sqrt(np.float32(d @ d), dtype=np.float32))
+    np.testing.assert_allclose(np.array(cam.front[:], np.float32), want, rtol=2e-7, atol=0)
+    v, _ = gcs.camera_matrices(cam, 640, 360)
+    eye = v @ np.append(target, np.float32(1.0)).astype(np.float64)
+    assert abs(eye[0]) < 1e-3 and abs(eye[1]) < 1e-3 and eye[2] < 0
+    with pytest.raises(gcs.GcsError):
+        gcs.camera_look_at(cam, cam.pos[:])
