@@ -86,6 +86,19 @@ def test_pinned_array_inside_a_block(gcs_mod, byte_offset):
     _pair(gcs, stars, [len(stars)], 32, _params(gcs), steps=2, pinned=True, byte_offset=byte_offset)
 
 
+@pytest.mark.parametrize("width,leaf,theta,pot", [(16, 1, 0.5, 0), (48, 32, 0.7, 0), (32, 4, 0.0, 0),
+                                                   (64, 8, 0.5, 1)])
+@pytest.mark.parametrize("pinned", [False, True])
+def test_overlapped_host_step_settings(gcs_mod, width, leaf, theta, pot, pinned):
+    """Other group widths (two targets a lane above 32), leaf sizes, theta 0
+    (every node opened) and potentials: the same bits as the plain step."""
+    gcs = gcs_mod
+    stars = small_collision(1500, 350, 150, seed=26)  # 4,000 particles
+    p = gcs.reference_params(theta=theta, epsilon_sq=0.05 ** 2, dt=0.005, leaf_size=leaf, walk_batch=64,
+                             bounds_mode=gcs.BOUNDS_DEVICE, com_fp64=1, with_potential=pot)
+    _pair(gcs, stars, [len(stars)], width, p, steps=2, pinned=pinned)
+
+
 def test_overlapped_host_step_many_chunks(gcs_mod):
     gcs = gcs_mod
     stars = small_collision(30000, 7000, 3000, seed=18)  # 80,000 particles: 2,500 groups, 48 chunks
