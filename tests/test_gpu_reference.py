@@ -15,7 +15,7 @@ import os
 import numpy as np
 import pytest
 
-from conftest import rel_err, small_collision
+from conftest import rel_err
 
 pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")

@@ -4,7 +4,6 @@ sorted particles (gcs_set_step_range), and the slices of the position and
 velocity arrays are exchanged after every step (the all-gather of a
 multi-GPU job, here device-to-device copies through gcs_device_array).
 Both contexts must then hold exactly the single-context state."""
-import numpy as np
 import pytest
 
 from conftest import small_collision
