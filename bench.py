@@ -47,6 +47,12 @@ THETA, EPS, DT = 0.5, 0.02, 0.0025
 FLOPS_PER_INTERACTION = 20
 WORKLOAD = ("two-galaxy collision, 1,048,576 particles (2 x [384,000 MN disc + 96,000 Hernquist bulge + "
             "44,288 Hernquist halo]), theta=0.5, eps=0.02, dt=0.0025, leaf<=32")
+L2_NOTE = "working set ~270 MB > 126 MB L2; no flush"
+
+
+def bench_config(n, world):
+    """The `config` object both arms print (the same workload on each)."""
+    return {"workload": WORKLOAD, "particles": n, "l2": L2_NOTE, "parallelism": "replicas x%d" % world}
 
 
 def parse():
@@ -764,11 +770,13 @@ def served_bench(gcs, torch, args, batched_rate):
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return 0
-    import gcs  # noqa: PLC0415
-    stars = gcs.collision_equal(*counts_for(args.n), seed=0)
-    n = len(stars)
+    # the scenario comes from the standalone generator library
+    # (oracle/_ref/libic.so, the same seeded recipe as the engine's own), so
+    # this arm loads no library of the engine
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle  # noqa: PLC0415
+    stars = oracle.collision_equal(*counts_for(args.n), seed=0)
+    n = len(stars)
     L = oracle.ref_lib("ref_cpu")
     if L is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_cpu.so not built"}))
@@ -789,7 +797,7 @@ def run_reference_arm(args, rank, world):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded two-galaxy initial conditions)", "impl": "reference",
-            "config": {"workload": WORKLOAD, "particles": n},
+            "config": bench_config(n, world),
             "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": cores, "kind": "reference",
                              "sample": "%d whole steps of the reference CPU Barnes-Hut (engine.cpp, "
                                        "gravity_aggregator.cpp, theta 0.5) after %d warm-up steps"
@@ -924,10 +932,9 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded two-galaxy initial conditions, seed = rank)",
-            "config": {"workload": WORKLOAD, "particles": n, "leaf_size": p.leaf_size,
-                       "walk_batch": p.walk_batch, "group_width": ctx.group_width, "autotuned": tuned,
-                       "com": "fp64 sums", "bounds": "device, per step",
-                       "l2": "working set ~270 MB > 126 MB L2; no flush", "parallelism": "replicas x%d" % world},
+            "config": bench_config(n, world),
+            "settings": {"leaf_size": p.leaf_size, "walk_batch": p.walk_batch, "group_width": ctx.group_width,
+                         "autotuned": tuned, "com": "fp64 sums", "bounds": "device, per step"},
             "e2e": e2e, "roofline": roofline, "clocks": clocks, "gpu_launches": launches_per_step * args.steps,
             "device_status": status}
     if rank == 0 and world == 1:

@@ -15,11 +15,31 @@
 //            walk work counter, device bounds)
 #pragma once
 #include <cstdint>
+#include <mutex>
+#include <utility>
 #include <cuda_runtime.h>
 #include "../../include/gcs_types.h"
 #include "../../include/gcs.h"
 
 namespace gcs {
+
+// ---- per-device set-up ------------------------------------------------------
+// Kernel attributes (the dynamic shared-memory opt-in above 48 KB) belong to
+// a device's context, not to the process: a process that drives several
+// devices must set them on each.  once_per_device runs `set` once for the
+// current device, thread-safe; devices beyond kMaxDevices run it every time.
+constexpr int kMaxDevices = 64;
+int current_device();      // the current device, or -1
+int current_sm_count();    // its SM count (cached per device; 148 if unknown)
+template <class F>
+void once_per_device(std::once_flag (&flags)[kMaxDevices], F&& set) {
+    const int dev = current_device();
+    if (dev < 0 || dev >= kMaxDevices) {
+        set();
+        return;
+    }
+    std::call_once(flags[dev], std::forward<F>(set));
+}
 
 constexpr int kRadixBits = 8;
 constexpr int kRadix = 1 << kRadixBits;

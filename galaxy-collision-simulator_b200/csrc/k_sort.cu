@@ -233,14 +233,11 @@ void launch_sort_pass(const Layout& L, int pass, const uint64_t* keys_in, const 
     if (L.n <= 0) return;
     const int64_t tiles = (L.n + kSortTile - 1) / kSortTile;
     const size_t smem = sizeof(SortSmem);
-    static bool configured = false;
-    if (!configured) {
-        cudaFuncSetAttribute(onesweep_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem);
-        cudaFuncSetAttribute(onesweep_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem);
-        configured = true;
-    }
+    static std::once_flag configured[kMaxDevices];
+    once_per_device(configured, [smem] {
+        cudaFuncSetAttribute(onesweep_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(onesweep_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    });
     uint32_t* lb = lookback + (size_t)pass * tiles * kRadix;
     if (pass < kKeyPasses) {
         onesweep_kernel<false><<<(unsigned)tiles, kSortThreads, smem, st>>>(

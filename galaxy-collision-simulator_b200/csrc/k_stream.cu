@@ -4,23 +4,38 @@
 //
 // All particle records are float4 (16-byte) loads/stores; grids are sized
 // as a multiple of the SM count with grid-stride loops.
+#include <atomic>
+
 #include "gcs_internal.h"
 #include "device_math.cuh"
 
 namespace gcs {
+
+int current_device() {
+    int dev = -1;
+    return cudaGetDevice(&dev) == cudaSuccess ? dev : -1;
+}
+
+int current_sm_count() {
+    static std::atomic<int> cached[kMaxDevices] = {};
+    const int dev = current_device();
+    if (dev >= 0 && dev < kMaxDevices) {
+        const int v = cached[dev].load(std::memory_order_relaxed);
+        if (v > 0) return v;
+    }
+    int sms = 0;
+    if (dev < 0 || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0)
+        sms = 148;
+    if (dev >= 0 && dev < kMaxDevices) cached[dev].store(sms, std::memory_order_relaxed);
+    return sms;
+}
 
 namespace {
 
 constexpr int kStreamThreads = 256;
 
 int stream_grid(int64_t n) {
-    static int sms = 0;
-    if (sms == 0) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms <= 0) sms = 148;
-    }
+    const int sms = current_sm_count();
     int64_t want = (n + kStreamThreads - 1) / kStreamThreads;
     int64_t cap = (int64_t)sms * 8;
     if (want > cap) want = cap;

@@ -62,6 +62,7 @@
 // the Star array is pinned host memory mapped into the device, the records
 // go straight into it and no chunk is counted (host_flags == nullptr).
 #include <algorithm>
+#include <atomic>
 
 #include "gcs_internal.h"
 #include "device_math.cuh"
@@ -716,15 +717,15 @@ constexpr size_t smem_bytes() {
     return sizeof(WarpSmem<H, T>) * kWalkWarps;
 }
 
-// Opt the instantiation in to its dynamic shared memory (above 48 KB).
+// Opt the instantiation in to its dynamic shared memory (above 48 KB), once
+// per device.
 template <int H, int T, bool kPot, bool kCount>
 void configure() {
-    static bool done = false;
-    if (!done) {
+    static std::once_flag done[kMaxDevices];
+    once_per_device(done, [] {
         cudaFuncSetAttribute(walk_kernel<H, T, kPot, kCount>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem_bytes<H, T>());
-        done = true;
-    }
+    });
 }
 
 template <int H, int T, bool kPot, bool kCount>
@@ -738,14 +739,18 @@ int occupancy_of() {
 
 template <int T>
 int max_blocks_of(int batch, int with_potential) {
-    // the same for every device of this build (sm_100a only)
-    static int cached[2][2] = {{0, 0}, {0, 0}};
+    // per device (the query needs the device's attribute opt-in first)
+    static std::atomic<int> cached[kMaxDevices][2][2] = {};
     const int hi = batch > 32 ? 1 : 0, pot = with_potential ? 1 : 0;
-    int& nb = cached[hi][pot];
-    if (nb == 0) {
-        if (hi) nb = pot ? occupancy_of<2, T, true, false>() : occupancy_of<2, T, false, false>();
-        else nb = pot ? occupancy_of<1, T, true, false>() : occupancy_of<1, T, false, false>();
+    const int dev = current_device();
+    if (dev >= 0 && dev < kMaxDevices) {
+        const int v = cached[dev][hi][pot].load(std::memory_order_relaxed);
+        if (v > 0) return v;
     }
+    int nb;
+    if (hi) nb = pot ? occupancy_of<2, T, true, false>() : occupancy_of<2, T, false, false>();
+    else nb = pot ? occupancy_of<1, T, true, false>() : occupancy_of<1, T, false, false>();
+    if (dev >= 0 && dev < kMaxDevices) cached[dev][hi][pot].store(nb, std::memory_order_relaxed);
     return nb;
 }
 

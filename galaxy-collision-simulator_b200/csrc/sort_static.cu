@@ -24,7 +24,11 @@
 //     on the array and corrupt each other;
 //   * the first call on a device looks up that device's address of the array
 //     (cudaGetSymbolAddress, with the device current) and keeps it; make that
-//     first call before any stream capture on the device.
+//     first call before any stream capture on the device;
+//   * with a caller status word the call only queues work on its stream; with
+//     status == NULL it waits for its stream to finish and reads the array's
+//     own status word, so that a look-back that gave up (a tile whose scatter
+//     was skipped) is returned as GCS_ERR_DEVICE instead of going unseen.
 #include <cstdio>
 #include <mutex>
 
@@ -51,7 +55,6 @@ static __device__ __align__(256) uint32_t g_sort_scratch[kScratchWords];
 
 namespace {
 
-constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 uint32_t* g_scratch_addr[kMaxDevices] = {};
 
@@ -116,9 +119,10 @@ extern "C" int gcs_sort_pairs_static(uint64_t* keys, uint32_t* vals, uint64_t* k
     const int64_t tiles = (n + kSortTile - 1) / kSortTile;
     const size_t clear_words = kHistWords + kTicketWords + kStatusWords + (size_t)tiles * kRadix * kKeyPasses;
     if (cudaMemsetAsync(base, 0, clear_words * sizeof(uint32_t), st) != cudaSuccess) return GCS_ERR_CUDA;
-    int grid = (int)((n + 255) / 256);
-    if (grid > 148 * 8) grid = 148 * 8;
-    key_histograms_kernel<<<grid, 256, 0, st>>>(keys, n, hist);
+    int64_t grid = (n + 255) / 256;
+    const int64_t cap = (int64_t)current_sm_count() * 8;  // 8 resident 256-thread blocks per SM
+    if (grid > cap) grid = cap;
+    key_histograms_kernel<<<(unsigned)grid, 256, 0, st>>>(keys, n, hist);
     Layout L;
     L.n = (int32_t)n;
     L.nseg = 1;
@@ -132,5 +136,13 @@ extern "C" int gcs_sort_pairs_static(uint64_t* keys, uint32_t* vals, uint64_t* k
         const int in = pass & 1;
         launch_sort_pass(L, pass, kb[in], vb[in], kb[in ^ 1], vb[in ^ 1], hist, tickets, lookback, stat, st);
     }
-    return cudaGetLastError() == cudaSuccess ? GCS_OK : GCS_ERR_CUDA;
+    if (cudaGetLastError() != cudaSuccess) return GCS_ERR_CUDA;
+    if (status) return GCS_OK;
+    // no caller status word: wait and read the array's own, so that a pass
+    // that gave up is reported (pageable destination: no allocation)
+    uint32_t seen = 0;
+    if (cudaMemcpyAsync(&seen, own_status, sizeof seen, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return GCS_ERR_CUDA;
+    return seen ? GCS_ERR_DEVICE : GCS_OK;
 }

@@ -299,8 +299,10 @@ int gcs_autotune(gcs_ctx* ctx, gcs_params* p, double* best_walk_ms);
  * synchronisation, or a plug-in whose host application owns the device
  * memory budget).  All pointers are device memory owned by the caller:
  * keys/vals hold the pairs and receive the sorted pairs; keys_alt/vals_alt
- * are the same length and are overwritten by the passes; status (may be
- * NULL) receives GCS_DEV_SORT_LOOKBACK_TIMEOUT if a pass gave up.  The
+ * are the same length and are overwritten by the passes; status (a device
+ * word) receives GCS_DEV_SORT_LOOKBACK_TIMEOUT if a pass gave up and the
+ * call only queues work on `stream`.  With status == NULL the call waits for
+ * `stream` and returns GCS_ERR_DEVICE if a pass gave up.  The
  * histograms and look-back state live in one static device array of about
  * 2.1 MB that every GPU loading this library keeps until exit; no call
  * allocates.  Each call clears that array on `stream` (a cudaStream_t, NULL
@@ -308,7 +310,7 @@ int gcs_autotune(gcs_ctx* ctx, gcs_params* p, double* best_walk_ms);
  * independent, but calls that overlap on the GPU race on it.  The first
  * call on a device looks up the array's device address (with that device
  * current) - make it before any stream capture.  Larger n returns
- * GCS_ERR_CAPACITY; the call is asynchronous. */
+ * GCS_ERR_CAPACITY. */
 int gcs_sort_pairs_static(uint64_t* keys, uint32_t* vals, uint64_t* keys_alt, uint32_t* vals_alt,
                           int64_t n, uint32_t* status, void* stream);
 /* FP64 direct-sum accelerations (excluding only i == j) at `n_targets`

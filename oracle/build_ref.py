@@ -2,9 +2,10 @@
 
 * ``build_oracle()`` compiles the C restatement ``oracle/gcs_oracle.c`` into
   ``oracle/liboracle.so`` (no FMA contraction, no fast-math).
-* ``build_ref()`` compiles the reference's own sources, where they lie under
-  ``/root/reference``, into ``oracle/_ref/`` (git-ignored, shipped to the GPU
-  box with the snapshot):
+* ``build_ref()`` compiles the reference's own sources, where they lie (the
+  directory named by the ``GCS_REFERENCE_DIR`` environment variable, else a
+  checkout named ``reference`` beside this repository), into ``oracle/_ref/``
+  (git-ignored, shipped with the built libraries):
 
   - ``libref_cuda.so``: the reference GPU engine (``cuda_engine.cu`` +
     ``karras_bvh.cuh`` + ``morton.h`` + CUB) for sm_100a, from a generated
@@ -31,7 +32,8 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
-REF = "/root/reference"
+# the reference checkout: $GCS_REFERENCE_DIR, else ../reference beside the repository
+REF = os.environ.get("GCS_REFERENCE_DIR") or os.path.join(os.path.dirname(REPO), "reference")
 OUT = os.path.join(HERE, "_ref")
 BUILD = os.path.join(OUT, "build")
 NVCC = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
@@ -57,6 +59,21 @@ def build_oracle(force: bool = False) -> str:
     if force or not _newer(lib, [src, hdr, __file__]):
         _run(["gcc", "-O2", "-std=c11", "-fPIC", "-shared", "-ffp-contract=off", "-fno-fast-math",
               src, "-o", lib, "-lm"])
+    return lib
+
+
+def build_ic(force: bool = False) -> str:
+    """The seeded initial-conditions generator (the package's host-only
+    ic_generator.cpp) as its own library, oracle/_ref/libic.so, so that
+    bench.py's reference arm builds the benchmark scenario without loading
+    the engine library (both arms step the identical particles)."""
+    src = os.path.join(REPO, "galaxy-collision-simulator_b200", "csrc", "ic_generator.cpp")
+    hdr = os.path.join(REPO, "include", "gcs.h")
+    lib = os.path.join(OUT, "libic.so")
+    if force or not _newer(lib, [src, hdr, __file__]):
+        os.makedirs(OUT, exist_ok=True)
+        _run(["g++", "-O3", "-std=c++17", "-fPIC", "-shared", "-pthread", "-I" + os.path.join(REPO, "include"),
+              src, "-o", lib, "-Wl,--no-undefined"])
     return lib
 
 
@@ -97,9 +114,11 @@ def _theta_aggregator() -> str:
 
 
 def build_ref(force: bool = False) -> dict:
-    """Build oracle/_ref from /root/reference; returns {name: path}. No-op
-    (returns existing libraries) when the reference is absent."""
+    """Build oracle/_ref from the reference checkout (and libic.so); returns
+    {name: path}.  Without the reference only libic.so is (re)built and the
+    existing reference libraries are returned."""
     libs = {k: os.path.join(OUT, "lib%s.so" % k) for k in ("ref_cuda", "ref_cpu", "ref_morton")}
+    libs["ic"] = build_ic(force)
     if not os.path.isdir(REF):
         return {k: v for k, v in libs.items() if os.path.exists(v)}
     os.makedirs(BUILD, exist_ok=True)

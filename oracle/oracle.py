@@ -223,6 +223,33 @@ def ref_lib(name: str):
     return L
 
 
+def collision_equal(n_disc: int, n_bulge: int, n_halo: int, seed: int = 0) -> np.ndarray:
+    """The equal-galaxy recipe's seeded initial conditions from
+    oracle/_ref/libic.so (the same generator source as the engine library's
+    gcs.collision_equal, built on its own so a caller need not load the
+    engine)."""
+    from gcs import CollisionSpec  # noqa: PLC0415  (ctypes layout only; loads no library)
+    path = os.path.join(REF_DIR, "libic.so")
+    if not os.path.exists(path):
+        from build_ref import build_ic  # noqa: PLC0415
+        build_ic()
+    L = C.CDLL(path)
+    L.gcs_collision_spec_equal.argtypes = [C.POINTER(CollisionSpec), _i64, _i64, _i64, _u64]
+    L.gcs_collision_spec_equal.restype = C.c_int
+    L.gcs_collision_count.argtypes = [C.POINTER(CollisionSpec)]
+    L.gcs_collision_count.restype = _i64
+    L.gcs_generate_collision.argtypes = [C.POINTER(CollisionSpec), _P, _i64]
+    L.gcs_generate_collision.restype = C.c_int
+    spec = CollisionSpec()
+    if L.gcs_collision_spec_equal(C.byref(spec), n_disc, n_bulge, n_halo, seed) != 0:
+        raise RuntimeError("collision spec rejected")
+    n = L.gcs_collision_count(C.byref(spec))
+    out = np.zeros(n, STAR_DTYPE)
+    if L.gcs_generate_collision(C.byref(spec), _ptr(out), n) != 0:
+        raise RuntimeError("initial-conditions generator failed")
+    return out
+
+
 def ref_initial_conditions(seed: int, num_dm: int, num_disc: int, num_bulge: int) -> np.ndarray:
     """The reference generator's own two-galaxy setup (generator.cpp:169-210), seeded."""
     L = ref_lib("ref_cpu")
