@@ -77,10 +77,10 @@ def parse():
     ap.add_argument("--batched-count", type=int, default=256)
     ap.add_argument("--batched-steps", type=int, default=10)
     ap.add_argument("--no-served", action="store_true")
-    ap.add_argument("--served-requests", type=int, default=48)
-    ap.add_argument("--served-step-scale", type=float, default=0.05)
-    ap.add_argument("--served-loads", type=lambda v: [float(x) for x in v.split(",")], default=[0.5, 0.9],
-                    help="offered loads as fractions of the batched throughput")
+    ap.add_argument("--served-requests", type=int, default=240)
+    ap.add_argument("--served-window", type=float, default=10.0, help="seconds served per load and mode")
+    ap.add_argument("--served-loads", type=lambda v: [float(x) for x in v.split(",")], default=[0.5, 1.0, 1.5, 2.0],
+                    help="offered loads as multiples of the one-at-a-time capacity")
     return ap.parse_args()
 
 
@@ -696,73 +696,119 @@ def batched_bench(gcs, torch, args):
             "ic_seconds": gen_s}
 
 
-def _serve(gcs, p, reqs, stars, max_segments, budget):
-    """Drive a server with requests arriving at their wall-clock times; returns
-    latencies (ms) and the makespan (first arrival to last completion)."""
+def _serve_window(gcs, p, reqs, stars, max_segments, budget, window_s):
+    """Drive a server for `window_s` seconds with requests arriving at their
+    wall-clock times: returns per-completed-request latencies (ms), the
+    particle-steps the server advanced over the window, its wall time (to the
+    last step's completion) and the peak residency."""
     srv = gcs.Server(p, max_particles=(1 << 30) - 1, max_segments=max_segments, hbm_budget_bytes=budget)
+    lat, queued = [], []
     try:
-        lat, queued = [], []
         t0 = time.perf_counter()
-        i, done, R = 0, 0, len(reqs)
-        peak = [0, 0]
-        while done < R:
+        i, R = 0, len(reqs)
+        while True:
             now = time.perf_counter() - t0
+            if now >= window_s:
+                break
             while i < R and reqs[i].arrival_s <= now:
                 srv.submit(i, stars[i], reqs[i].steps)
                 i += 1
-            q, r, f = srv.counts()
-            if q + r == 0 and f == 0:
-                if i < R:
-                    time.sleep(max(0.0, min(0.001, reqs[i].arrival_s - now)))
-                continue
+            q, r, _ = srv.counts()
             if q + r:
-                res = srv.tick()
-                peak = [max(peak[0], res[0]), max(peak[1], res[1])]
+                srv.tick()
+            elif i < R:
+                time.sleep(max(0.0, min(0.001, reqs[i].arrival_s - now)))
             while (x := srv.pop(with_stars=False)) is not None:
                 info = x[0]
                 if info.status != 0:
                     raise RuntimeError("served scenario %d failed with status %d" % (info.id, info.status))
                 lat.append(info.latency_ms)
                 queued.append(info.queued_ms)
-                done += 1
-        makespan = time.perf_counter() - t0 - reqs[0].arrival_s
-        cap = srv.capacity
+        # the steps still queued count in the progress: wait for them
+        srv.L.gcs_synchronize(srv.L.gcs_server_context(srv._h))
+        t_end = time.perf_counter()
+        advanced, steps, peak_sc, peak_n = srv.progress()
+        counts = srv.counts()
     finally:
         srv.close()
-    return lat, queued, makespan, peak, cap
+    return {"arrived": i, "completed": len(lat), "queued_at_end": counts[0], "resident_at_end": counts[1],
+            "p50_ms": float(np.percentile(lat, 50)) if lat else None,
+            "p99_ms": float(np.percentile(lat, 99)) if lat else None,
+            "mean_queue_ms": float(np.mean(queued)) if queued else None,
+            "throughput": advanced / (t_end - t0), "unit": "particle-steps/s", "seconds": t_end - t0,
+            "server_steps": steps, "peak_resident_scenarios": peak_sc, "peak_resident_particles": peak_n}
 
 
-def served_bench(gcs, torch, args, batched_rate):
-    """Poisson request streams at offered loads that are fractions of the
-    batched throughput, served by continuous batching and by the plain
-    one-at-a-time path (the same server with one slot)."""
+def plain_step_ms(gcs, torch, p, sizes, steps=8):
+    """Device time of one step of one scenario alone (one segment, graph-
+    captured step), per particle count: the one-at-a-time path's rate."""
+    stream = torch.cuda.Stream()
+    out = {}
+    with gcs.Context(max(sizes)) as ctx:
+        ctx.set_stream(stream.cuda_stream)
+        ctx.set_graphs(True)
+        for n in sizes:
+            st = gcs.collision_pair(n, 0.6, 7.5, 0.55, 45.0, seed=n)
+            ctx.set_segments([n])
+            ctx.upload(st)
+            for _ in range(3):
+                ctx.step(p)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                ctx.step(p)
+            e1.record(stream)
+            e1.synchronize()
+            out[n] = e0.elapsed_time(e1) / steps
+        if ctx.device_status():
+            raise RuntimeError("device status raised in the per-size runs")
+    return out
+
+
+def served_bench(gcs, torch, args):
+    """Poisson request streams (unscaled step counts) at offered loads that
+    are multiples of the one-at-a-time capacity, served for a fixed window by
+    continuous batching and by the plain one-at-a-time path (the same server
+    with one slot, FIFO).  The one-at-a-time capacity of the stream comes from
+    measured per-size step times: sum(N * steps) / sum(steps * t_step(N))."""
     import workloads  # noqa: PLC0415
     free, _ = torch.cuda.mem_get_info()
     budget = min(150e9, 0.8 * free)
-    base = workloads.serving_requests(args.served_requests, 1.0, step_scale=args.served_step_scale)
+    base = workloads.serving_requests(args.served_requests, 1.0)
+    t0 = time.perf_counter()
     stars = [s.stars(gcs) for s in base]
-    work = [s.n * s.steps for s in base]
-    mean_work = float(np.mean(work))
+    gen_s = time.perf_counter() - t0
     p = make_params(gcs, 8, 0)
     with gcs.Context(max(len(s) for s in stars)) as ctx:
         ctx.upload(stars[int(np.argmax([len(s) for s in stars]))])
         p = _tune(gcs, ctx)
+    sizes = [8192, 16384, 32768, 65536, 131072, 262144, 524288, 1048576]
+    t_ms = plain_step_ms(gcs, torch, p, sizes)
+    ln = np.log(np.array(sizes, float))
+    tt = np.array([t_ms[n] for n in sizes])
+
+    def t_step(n):
+        return float(np.interp(np.log(n), ln, tt))
+
+    work = np.array([s.n * s.steps for s in base], float)
+    cap1 = float(work.sum() / sum(s.steps * t_step(s.n) / 1e3 for s in base))
     out = {"workload": "%d requests, Poisson arrivals, N log-uniform in [8192, 1048576], steps uniform in "
-                       "[100, 2000] x %.3g, other draws as the batched stream; theta=0.5, eps=0.02, dt=0.0025"
-                       % (len(base), args.served_step_scale),
-           "hbm_budget_bytes": budget, "leaf_size": p.leaf_size, "loads": []}
+                       "[100, 2000] (unscaled), other draws as the batched stream; theta=0.5, eps=0.02, dt=0.0025"
+                       % len(base),
+           "window_s": args.served_window, "hbm_budget_bytes": budget, "leaf_size": p.leaf_size,
+           "ic_seconds": gen_s,
+           "plain_step_ms": {str(n): t_ms[n] for n in sizes},
+           "one_at_a_time_capacity": cap1,
+           "capacity_note": "sum(N*steps)/sum(steps*t_step(N)) over the stream, t_step from the per-size runs",
+           "loads": []}
+    mean_work = float(work.mean())
     for rho in args.served_loads:
-        rate = rho * batched_rate / mean_work
-        reqs = workloads.serving_requests(args.served_requests, rate, step_scale=args.served_step_scale)
-        row = {"offered_fraction_of_batched_throughput": rho, "rate_req_per_s": rate,
-               "offered_particle_steps_per_s": rate * mean_work}
+        rate = rho * cap1 / mean_work
+        reqs = workloads.serving_requests(args.served_requests, rate)
+        row = {"offered_load": rho, "rate_req_per_s": rate, "offered_particle_steps_per_s": rate * mean_work}
         for name, slots in (("continuous_batching", 256), ("one_at_a_time", 1)):
-            lat, qd, span, peak, cap = _serve(gcs, p, reqs, stars, slots, budget)
-            row[name] = {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-                         "mean_queue_ms": float(np.mean(qd)),
-                         "throughput": float(sum(work) / span), "unit": "particle-steps/s",
-                         "makespan_s": span, "peak_resident_scenarios": peak[0],
-                         "peak_resident_particles": peak[1], "capacity_particles": cap}
+            row[name] = _serve_window(gcs, p, reqs, stars, slots, budget, args.served_window)
+        row["throughput_ratio"] = row["continuous_batching"]["throughput"] / row["one_at_a_time"]["throughput"]
         out["loads"].append(row)
     return out
 
@@ -954,8 +1000,7 @@ def main():
         if not args.no_batched:
             line["batched"] = batched_bench(gcs, torch, args)
         if not args.no_served:
-            rate = line["batched"]["batched"]["value"] if "batched" in line else value
-            line["served"] = served_bench(gcs, torch, args, rate)
+            line["served"] = served_bench(gcs, torch, args)
     if rank == 0:
         print(json.dumps(line))
     if dist is not None:

@@ -63,6 +63,13 @@ struct gcs_ctx {
     int64_t* seg_off = nullptr;
     int32_t* seg_id = nullptr;
     WalkGroup* groups = nullptr;
+    // walk frontiers: super-groups of consecutive groups, their lists
+    SuperGroup* supers = nullptr;
+    int32_t* sg_list = nullptr;
+    int32_t* sg_src = nullptr;
+    int4* sg_meta = nullptr;
+    int n_supers = 0;
+    size_t supers_cap = 0;
     Chunk* chunks = nullptr;
     float2* seg_bounds = nullptr;
     Star* staging = nullptr;
@@ -100,6 +107,7 @@ struct gcs_ctx {
     uint32_t star_epoch = 0;
     size_t walk_stack_entries = 0;
     int32_t group_width = 32;              // targets per walk group (<= 64; two per lane above 32)
+    bool walk_frontier = true;             // super-group frontier pass before the walk
     // particles the walk and the kick/drift cover (sorted order; count < 0:
     // all): one rank's slice when one scenario is stepped across devices
     int64_t range_first = 0;
@@ -223,7 +231,8 @@ void free_all(gcs_ctx* c) {
     if (c->star_flags) cudaFreeHost(c->star_flags);
     void* ptrs[] = {c->pos[0], c->pos[1], c->vel[0], c->vel[1], c->acc, c->keys[0], c->keys[1],
                     c->idx[0], c->idx[1], c->tr, c->bd, c->wn, c->com64, c->leaf_parent, c->seg_off,
-                    c->seg_id, c->groups, c->chunks, c->seg_bounds, c->staging, c->pb_staging,
+                    c->seg_id, c->groups, c->supers, c->sg_list, c->sg_src, c->sg_meta, c->chunks,
+                    c->seg_bounds, c->staging, c->pb_staging,
                     c->scratch, c->status, c->diag, c->targets, c->direct_out, c->counts,
                     c->walk_stack, c->render_acc, c->render_rgba, c->star_chunk_done};
     for (void* p : ptrs)
@@ -278,23 +287,41 @@ bool range_boundary_ok(const gcs_ctx* c, int64_t b) {
     return false;
 }
 
+// Groups per super-group for a group width: whole groups of at most
+// kSuperTargets targets (at least one group).
+int groups_per_super(int width) { return std::max(1, kSuperTargets / width); }
+
 int upload_groups(gcs_ctx* c) {
     std::vector<WalkGroup> groups;
+    std::vector<SuperGroup> supers;
     groups.reserve((size_t)(c->n / c->group_width + c->nseg + 1));
     const int64_t rf = range_first(c), rl = rf + range_count(c);
+    const int per = groups_per_super(c->group_width);
     for (int s = 0; s < c->nseg; ++s) {
         const int64_t a = c->h_seg_off[s], e = c->h_seg_off[s + 1];
+        int in_super = per;  // groups in the current super-group (a segment starts a new one)
         for (int64_t g = a; g < e; g += c->group_width) {
             if (g < rf || g >= rl) continue;  // outside this context's step range
             WalkGroup w;
             w.start = (int32_t)g;
             w.count = (int32_t)std::min<int64_t>(c->group_width, e - g);
             w.seg = s;
-            w.pad = 0;
+            if (in_super == per) {
+                SuperGroup sg;
+                sg.start = w.start;
+                sg.count = 0;
+                sg.seg = s;
+                sg.pad = 0;
+                supers.push_back(sg);
+                in_super = 0;
+            }
+            supers.back().count += w.count;
+            ++in_super;
+            w.super = (int32_t)supers.size() - 1;
             groups.push_back(w);
         }
     }
-    if (groups.size() > c->groups_cap) {
+    if (groups.size() > c->groups_cap || supers.size() > c->supers_cap) {
         c->last_error = "group table capacity exceeded";
         return GCS_ERR_CAPACITY;
     }
@@ -302,6 +329,10 @@ int upload_groups(gcs_ctx* c) {
     GCS_CUDA(c, cudaStreamSynchronize(c->stream));
     GCS_CUDA(c, cudaMemcpyAsync(c->groups, groups.data(), sizeof(WalkGroup) * groups.size(),
                                 cudaMemcpyHostToDevice, c->stream));
+    if (!supers.empty())
+        GCS_CUDA(c, cudaMemcpyAsync(c->supers, supers.data(), sizeof(SuperGroup) * supers.size(),
+                                    cudaMemcpyHostToDevice, c->stream));
+    c->n_supers = (int)supers.size();
     c->n_groups = (int)groups.size();
     c->h_group_start.resize(groups.size());
     for (size_t g = 0; g < groups.size(); ++g) c->h_group_start[g] = groups[g].start;
@@ -333,9 +364,15 @@ static int walk_stage(gcs_ctx* c, const gcs_params* p, const WalkEpilogue& ep) {
         c->wn_G = wnp.G;
         c->wn_L = wnp.leaf_size;
     }
+    WalkFrontier fr;
+    fr.supers = c->walk_frontier ? c->supers : nullptr;
+    fr.n_supers = c->n_supers;
+    fr.list = c->sg_list;
+    fr.src = c->sg_src;
+    fr.meta = c->sg_meta;
     launch_walk(L, wp, c->pos[c->cur], c->wn, c->groups, c->n_groups, c->group_width > 32 ? 2 : 1, c->acc,
                 scratch_at<uint32_t>(c, sl.walk_q), c->status, p->walk_blocks_per_sm, c->sm_count,
-                c->count_walk ? c->counts : nullptr, c->walk_stack, c->walk_stack_entries, st, ep);
+                c->count_walk ? c->counts : nullptr, c->walk_stack, c->walk_stack_entries, st, ep, fr);
     return check_launch(c, "walk");
 }
 
@@ -560,6 +597,15 @@ static int allocate_state(gcs_ctx* c) {
     if (!rc) rc |= dalloc(c, &c->seg_off, (size_t)max_segments + 1);
     if (!rc) rc |= dalloc(c, &c->seg_id, N);
     if (!rc) rc |= dalloc(c, &c->groups, max_groups);
+    // super-groups: full ones hold more than kSuperTargets - kGroupSize
+    // targets; a segment (or a step range within it) ends at most one
+    // partial one
+    const size_t max_supers = N / (size_t)(kSuperTargets - kGroupSize) + (size_t)max_segments + 1;
+    c->supers_cap = max_supers;
+    if (!rc) rc |= dalloc(c, &c->supers, max_supers);
+    if (!rc) rc |= dalloc(c, &c->sg_list, max_supers * (size_t)kSuperCap);
+    if (!rc) rc |= dalloc(c, &c->sg_src, max_supers * (size_t)kSuperSrcCap);
+    if (!rc) rc |= dalloc(c, &c->sg_meta, max_supers);
     if (!rc) rc |= dalloc(c, &c->chunks, max_chunks);
     if (!rc) rc |= dalloc(c, &c->seg_bounds, (size_t)max_segments);
     if (!rc) rc |= dalloc(c, &c->staging, N);
@@ -727,6 +773,13 @@ int gcs_set_group_width(gcs_ctx* c, int32_t width) {
 }
 
 int32_t gcs_group_width(const gcs_ctx* c) { return c ? c->group_width : 0; }
+
+int gcs_set_walk_frontier(gcs_ctx* c, int32_t enable) {
+    if (!c) return GCS_ERR_ARG;
+    if (c->walk_frontier != (enable != 0)) drop_graphs(c);
+    c->walk_frontier = enable != 0;
+    return GCS_OK;
+}
 
 int64_t gcs_num_particles(const gcs_ctx* c) { return c ? c->n : 0; }
 int32_t gcs_num_segments(const gcs_ctx* c) { return c ? c->nseg : 0; }

@@ -50,12 +50,13 @@ constexpr int kSortItems = 16;
 constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys per tile
 constexpr int kGroupSize = 64;         // walk targets per warp group (two per lane above 32)
 
-// Work unit of the walk: up to kGroupSize consecutive sorted particles of one segment.
+// Work unit of the walk: up to kGroupSize consecutive sorted particles of one
+// segment; `super` is its super-group (walk frontiers, below).
 struct WalkGroup {
     int32_t start;
     int32_t count;
     int32_t seg;
-    int32_t pad;
+    int32_t super;
 };
 
 // Per-segment bounds chunk: a range of particles of one segment.
@@ -191,11 +192,45 @@ constexpr int kMaxStarTailChunks = 48;
 constexpr int kMaxStarChunks = kMaxStarHeadChunks + kMaxStarTailChunks;
 constexpr int kWalkBlockWarps = 8;  // warps per walk block
 
+// ---- walk frontiers ------------------------------------------------------
+// Consecutive walk groups of one segment form a super-group of at most
+// kSuperTargets targets.  Before the walk, a frontier pass walks the tree once
+// per super-group against the super-group's bounding box (the same box test
+// as the group walk, which never contradicts a target's own opening test):
+// nodes every target of the super-group accepts go to its take list, the
+// particles of nodes every target opens and sums directly (leaf children,
+// small nodes) to its source list, the children of other nodes every target
+// opens are visited, and nodes the box cannot decide end the pass as its
+// frontier.  Every target of the super-group reaches each of those nodes with
+// every ancestor opened, so a group's walk evaluates the take list and the
+// sources for all its targets and then starts from the frontier with full
+// masks: each target's terms are exactly those of its walk from the root.
+// A super-group whose lists do not fit (kSuperCap, kSuperSrcCap) is marked
+// invalid and its groups walk from the root.
+constexpr int kSuperTargets = 256;
+constexpr int kSuperCap = 2048;     // take nodes (from the front) + frontier nodes (from the back)
+constexpr int kSuperSrcCap = 64;    // particle sources of a super-group
+// Targets [start, start + count) of segment seg (a run of whole groups).
+struct SuperGroup {
+    int32_t start;
+    int32_t count;
+    int32_t seg;
+    int32_t pad;
+};
+struct WalkFrontier {
+    const SuperGroup* supers = nullptr;  // null: every group walks from its root
+    int n_supers = 0;
+    int32_t* list = nullptr;  // [n_supers][kSuperCap]
+    int32_t* src = nullptr;   // [n_supers][kSuperSrcCap] sorted particle indices
+    int4* meta = nullptr;     // per super-group: n_take, n_src, n_front, valid
+};
+
 void launch_walk(const Layout& L, const WalkParams& wp, const float4* pos,
                  const WalkNode* wn, const WalkGroup* groups, int n_groups, int targets_per_lane,
                  float4* acc, uint32_t* queue, uint32_t* status, int blocks_per_sm,
                  int sm_count, unsigned long long* counts, int2* gstack, size_t gstack_entries,
-                 cudaStream_t st, const WalkEpilogue& ep = WalkEpilogue());
+                 cudaStream_t st, const WalkEpilogue& ep = WalkEpilogue(),
+                 const WalkFrontier& fr = WalkFrontier());
 int walk_max_blocks_per_sm(int batch, int with_potential, int targets_per_lane);
 // Persistent walk grid (blocks) for n_groups groups, and the global stack
 // entries that grid needs.

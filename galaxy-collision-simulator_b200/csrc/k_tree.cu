@@ -112,6 +112,9 @@ struct ChildData {
     double md;    // FP64 mass sum
 };
 
+// Loads child c; its FP64 sums only when `fp64` (the caller's test that c is
+// an internal node of at least kComFp64Min particles under a node that sums
+// in FP64; a particle is never one).
 __device__ __forceinline__ ChildData load_child(int c, int n_internal, const float4* __restrict__ pos,
                                                 const BvhNodeTraverse* tr, const BvhNodeBuild* bd,
                                                 const double4* com64, bool fp64) {
@@ -120,10 +123,6 @@ __device__ __forceinline__ ChildData load_child(int c, int n_internal, const flo
         const float4 p = __ldg(pos + (c - n_internal));
         r.lo = r.hi = r.com = make_float3(p.x, p.y, p.z);
         r.m = p.w;
-        if (fp64) {
-            r.md = p.w;
-            r.mx = make_double3((double)p.w * p.x, (double)p.w * p.y, (double)p.w * p.z);
-        }
     } else {
         // Written by another thread of this launch: read through L2.
         const float4 a = __ldcg(reinterpret_cast<const float4*>(tr + c));
@@ -144,13 +143,19 @@ __device__ __forceinline__ ChildData load_child(int c, int n_internal, const flo
 }
 
 constexpr int kAggThreads = 256;
+// FP64 centre-of-mass sums (com_fp64) are kept for the top of the tree:
+// nodes of at least this many particles, where the mass-weighted positions
+// of many particles are summed.  A child below the size (or a particle)
+// enters its parent's sums as the exact double product of its FP32 mass and
+// centre of mass (position).  Block-local nodes hold at most kAggThreads
+// particles, so they are never FP64 nodes.
+constexpr int kComFp64Min = 1024;
+static_assert(kComFp64Min > kAggThreads, "block-local nodes are never FP64 nodes");
 
 // A node finished inside the block, kept in shared memory for its parent.
 struct LocalNode {
     float3 lo, hi, com;
     float m;
-    double3 mx;
-    double md;
 };
 
 __device__ __forceinline__ ChildData from_local(const LocalNode& q) {
@@ -159,9 +164,19 @@ __device__ __forceinline__ ChildData from_local(const LocalNode& q) {
     r.hi = q.hi;
     r.com = q.com;
     r.m = q.m;
-    r.mx = q.mx;
-    r.md = q.md;
     return r;
+}
+
+// A child's terms in its parent's FP64 sums: its own sums if it is an FP64
+// node, else the double product of its FP32 mass and centre of mass.
+__device__ __forceinline__ void fp64_terms(const ChildData& c, bool big, double3& mx, double& md) {
+    if (big) {
+        mx = c.mx;
+        md = c.md;
+    } else {
+        md = (double)c.m;
+        mx = make_double3(md * (double)c.com.x, md * (double)c.com.y, md * (double)c.com.z);
+    }
 }
 
 // Walk record of internal node `node` (links already range-checked): the
@@ -236,7 +251,7 @@ aggregate_kernel(Layout L, const float4* __restrict__ pos,
     // The node this thread has just finished (first the leaf itself) is
     // carried in registers; at each parent only the sibling is loaded.
     int from = L.n_internal + g;
-    ChildData mine = load_child(from, L.n_internal, pos, tr, bd, com64, fp64);
+    ChildData mine = load_child(from, L.n_internal, pos, tr, bd, com64, false);
     int node = __ldg(leaf_parent + g);
     // Links come from the build launch, so they can be read at any time: the
     // first node's before the climb, each parent's as soon as the climb is
@@ -294,6 +309,13 @@ aggregate_kernel(Layout L, const float4* __restrict__ pos,
         }
         const bool left = cl == from;
         const int sib = left ? cr : cl;
+        // particles of the node and of its two children (the split is the
+        // left child's end of the range)
+        const int lo_p = min(own, re), hi_p = max(own, re);
+        const int split = cl >= L.n_internal ? cl - L.n_internal : cl + s;
+        const bool big = fp64 && hi_p - lo_p + 1 >= kComFp64Min;
+        const bool big_l = big && split - lo_p + 1 >= kComFp64Min;
+        const bool big_r = big && hi_p - split >= kComFp64Min;
         // a local node's internal children are local too: read them from
         // shared memory (their own range end is inside the block)
         ChildData other;
@@ -305,7 +327,7 @@ aggregate_kernel(Layout L, const float4* __restrict__ pos,
             }
             other = from_local(snode[so]);
         } else {
-            other = load_child(sib, L.n_internal, pos, tr, bd, com64, fp64);
+            other = load_child(sib, L.n_internal, pos, tr, bd, com64, left ? big_r : big_l);
         }
         const ChildData& A = left ? mine : other;   // left child
         const ChildData& B = left ? other : mine;   // right child
@@ -321,9 +343,13 @@ aggregate_kernel(Layout L, const float4* __restrict__ pos,
         next.md = 0.0;
         next.mx = make_double3(0.0, 0.0, 0.0);
         if (m > 0.0f) {
-            if (fp64) {
-                next.md = A.md + B.md;
-                next.mx = make_double3(A.mx.x + B.mx.x, A.mx.y + B.mx.y, A.mx.z + B.mx.z);
+            if (big) {
+                double3 amx, bmx;
+                double amd, bmd;
+                fp64_terms(A, big_l, amx, amd);
+                fp64_terms(B, big_r, bmx, bmd);
+                next.md = amd + bmd;
+                next.mx = make_double3(amx.x + bmx.x, amx.y + bmx.y, amx.z + bmx.z);
                 com = make_float3((float)(next.mx.x / next.md), (float)(next.mx.y / next.md),
                                   (float)(next.mx.z / next.md));
             } else {
@@ -336,7 +362,7 @@ aggregate_kernel(Layout L, const float4* __restrict__ pos,
                               __fmul_rn(__fadd_rn(lo.y, hi.y), 0.5f),
                               __fmul_rn(__fadd_rn(lo.z, hi.z), 0.5f));
         }
-        if (fp64) com64[node] = make_double4(next.mx.x, next.mx.y, next.mx.z, next.md);
+        if (big) com64[node] = make_double4(next.mx.x, next.mx.y, next.mx.z, next.md);
         float4* t4 = reinterpret_cast<float4*>(tr + node);
         t4[0] = make_float4(com.x, com.y, com.z, m);
         tr[node].width = width;
@@ -354,8 +380,6 @@ aggregate_kernel(Layout L, const float4* __restrict__ pos,
             q.hi = hi;
             q.com = com;
             q.m = m;
-            q.mx = next.mx;
-            q.md = next.md;
         }
         mine = next;
         from = node;

@@ -88,6 +88,30 @@ constexpr int kClassTakeFull = 4;  // kClassTake, and every live target is in it
 constexpr float kBoxLo = 1.0f - 1.0f / 65536.0f;
 constexpr float kBoxHi = 1.0f + 1.0f / 65536.0f;
 
+// Class of a node (centre of mass c, width^2 w2) against a box of targets:
+// the squared softened distances from c to the nearest and farthest points
+// of the box bound every target's own d2, and the 2^-16 margins in k_take =
+// theta^2 (1 - 2^-16) and k_open = theta^2 (1 + 2^-16) are far above the
+// few-ulp rounding of a target's own d2, so "take" means every target of the
+// box accepts the node (w2 < theta^2 d2) and "open" that every target opens
+// it.
+__device__ __forceinline__ int box_class(float4 c, float w2, float3 lo, float3 hi, float eps2, float k_take,
+                                         float k_open) {
+    float s2min = eps2, s2max = eps2;
+    const float dl[3] = {lo.x - c.x, lo.y - c.y, lo.z - c.z};
+    const float dh[3] = {c.x - hi.x, c.y - hi.y, c.z - hi.z};
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+        const float near = fmaxf(fmaxf(dl[ax], dh[ax]), 0.0f);
+        const float far = fmaxf(fabsf(dl[ax]), fabsf(dh[ax]));
+        s2min = fmaf(near, near, s2min);
+        s2max = fmaf(far, far, s2max);
+    }
+    if (w2 < s2min * k_take) return kClassTake;
+    if (w2 >= s2max * k_open) return kClassOpen;
+    return kClassMixed;
+}
+
 // Stack entry: node index and one lane mask per target slot.
 template <int T>
 struct EntryOf;
@@ -286,7 +310,8 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
             const WalkNode* __restrict__ wn, const WalkGroup* __restrict__ groups,
             int n_groups, float4* __restrict__ acc, uint32_t* __restrict__ queue,
             uint32_t* __restrict__ status, unsigned long long* __restrict__ counts,
-            typename EntryOf<T>::type* __restrict__ gstack, int gstack_cap, WalkEpilogue ep) {
+            typename EntryOf<T>::type* __restrict__ gstack, int gstack_cap, WalkEpilogue ep,
+            WalkFrontier fr) {
     using Smem = WarpSmem<H, T>;
     using Entry = typename Smem::Entry;
     extern __shared__ __align__(16) unsigned char walk_smem[];
@@ -349,8 +374,63 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
         int nsrc = 0;
 
         if (seg_n >= 2) {
-            int top = 1, gtop = 0;
-            if (lane == 0) W.stk[0] = make_entry(off - s, live);
+            int top = 0, gtop = 0;
+            int4 fm = make_int4(0, 0, 0, 0);
+            if (fr.meta) fm = fr.meta[grp.super];
+            if (fm.w && fm.z - Smem::kSpillAbove <= gstack_cap) {
+                // the super-group's shared work: its take list for every
+                // target (two records per lane per chunk of 64, staged in the
+                // source pairs), its sources, then the frontier as the stack
+                const int32_t* tl = fr.list + (size_t)grp.super * kSuperCap;
+                for (int base = 0; base < fm.x; base += kSrcCap) {
+                    const int cnt = min(kSrcCap, fm.x - base);
+                    const int padded = (cnt + 1) & ~1;
+                    for (int e = lane; e < padded; e += 32) {
+                        float4 q = make_float4(1e30f, 1e30f, 1e30f, 0.0f);
+                        if (e < cnt) q = __ldg(&wn[__ldg(tl + base + e)].cm);
+                        put_pair(W.sxy, W.szm, e, q);
+                    }
+                    __syncwarp();
+#pragma unroll 4
+                    for (int q = 0; q < (padded >> 1); ++q) {
+                        const float4 zm = W.szm[q];
+                        const float4 xy = W.sxy[q];
+#pragma unroll
+                        for (int t = 0; t < T; ++t) {
+                            const PairD d = pair_d_take(xy, zm, X.npx[t], X.npy[t], X.npz[t], e2);
+                            pair_add<kPot>(A[t], d, zm, true, true);
+                        }
+                    }
+                    __syncwarp();
+                }
+                if (kCount) {
+#pragma unroll
+                    for (int t = 0; t < T; ++t)
+                        if (valid[t]) A[t].n_mono += (uint32_t)fm.x;
+                    WC.w_node += (uint32_t)fm.x;
+                    WC.all_take += (uint32_t)fm.x;
+                }
+                if (fm.y > 0) {
+                    const int32_t* sl = fr.src + (size_t)grp.super * kSuperSrcCap;
+                    for (int e = lane; e < fm.y; e += 32) {
+                        W.srcp[e] = __ldg(sl + e);
+#pragma unroll
+                        for (int t = 0; t < T; ++t) W.srcm[t][e] = live[t];
+                    }
+                    flush_sources<H, T, kPot, kCount>(W, fm.y, lane, lane_bit, pos, G, X, e2, leaf_thr, A, WC);
+                }
+                // frontier entries [kSuperCap - n_front, kSuperCap): what the
+                // shared stack cannot hold goes to the global bottom
+                const int32_t* fl = tl + kSuperCap - fm.z;
+                const int to_g = max(0, fm.z - Smem::kSpillAbove);
+                for (int j = lane; j < to_g; j += 32) gstk[j] = make_entry(__ldg(fl + j), live);
+                for (int j = lane; j < fm.z - to_g; j += 32) W.stk[j] = make_entry(__ldg(fl + to_g + j), live);
+                gtop = to_g;
+                top = fm.z - to_g;
+            } else {
+                if (lane == 0) W.stk[0] = make_entry(off - s, live);
+                top = 1;
+            }
             __syncwarp();
             // Each internal node has one parent, so a walk pops it at most
             // once: more pops than internal nodes means a malformed tree.
@@ -406,23 +486,8 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                         bool full = true;
 #pragma unroll
                         for (int t = 0; t < T; ++t) full = full && my_mask[h][t] == live[t];
-                        // squared softened distances from the centre of mass
-                        // to the nearest and farthest points of the box
-                        float s2min = eps2, s2max = eps2;
-                        {
-                            const float dl[3] = {box_lo.x - a.x, box_lo.y - a.y, box_lo.z - a.z};
-                            const float dh[3] = {a.x - box_hi.x, a.y - box_hi.y, a.z - box_hi.z};
-#pragma unroll
-                            for (int ax = 0; ax < 3; ++ax) {
-                                const float near = fmaxf(fmaxf(dl[ax], dh[ax]), 0.0f);
-                                const float far = fmaxf(fabsf(dl[ax]), fabsf(dh[ax]));
-                                s2min = fmaf(near, near, s2min);
-                                s2max = fmaf(far, far, s2max);
-                            }
-                        }
-                        if (w2[h] < s2min * k_take) cls[h] = full ? kClassTakeFull : kClassTake;
-                        else if (w2[h] >= s2max * k_open) cls[h] = kClassOpen;
-                        else cls[h] = kClassMixed;
+                        cls[h] = box_class(a, w2[h], box_lo, box_hi, eps2, k_take, k_open);
+                        if (cls[h] == kClassTake && full) cls[h] = kClassTakeFull;
                     }
                 }
                 // compact into three pair-interleaved lists, each starting at
@@ -712,6 +777,126 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
     }
 }
 
+// Frontier pass (WalkFrontier, gcs_internal.h): one warp per super-group
+// walks the tree against the super-group's bounding box, 32 nodes per round
+// (lane k classifies node k with box_class).  Certified take nodes are
+// appended to the take list, undecided ones to the frontier, and nodes every
+// target opens contribute their internal children to the stack and their
+// particles (leaf children, or the whole range of a small node) to the
+// source list, in the order the group walk would use them.  Lists grow at
+// offsets from warp ballots and scans; a list or stack that would overflow,
+// or more pops than the segment has internal nodes, marks the super-group
+// invalid (its groups then walk from the root), so nothing is written out of
+// bounds.
+constexpr int kFrontWarps = 8;
+constexpr int kFrontStack = 1024;
+
+__global__ void __launch_bounds__(kFrontWarps * 32)
+frontier_kernel(Layout L, const float4* __restrict__ pos, const WalkNode* __restrict__ wn, WalkFrontier fr,
+                float eps2, float theta2, uint32_t* __restrict__ status) {
+    __shared__ int32_t stk_all[kFrontWarps][kFrontStack];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int sgi = blockIdx.x * kFrontWarps + warp;
+    if (sgi >= fr.n_supers) return;
+    int32_t* stk = stk_all[warp];
+    const uint32_t lt = (1u << lane) - 1u;
+    const SuperGroup sg = fr.supers[sgi];
+    float3 lo = make_float3(INFINITY, INFINITY, INFINITY), hi = make_float3(-INFINITY, -INFINITY, -INFINITY);
+    for (int i = lane; i < sg.count; i += 32) {
+        const float4 p = __ldg(pos + sg.start + i);
+        lo = make_float3(fminf(lo.x, p.x), fminf(lo.y, p.y), fminf(lo.z, p.z));
+        hi = make_float3(fmaxf(hi.x, p.x), fmaxf(hi.y, p.y), fmaxf(hi.z, p.z));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        lo.x = fminf(lo.x, __shfl_xor_sync(kFull, lo.x, o));
+        lo.y = fminf(lo.y, __shfl_xor_sync(kFull, lo.y, o));
+        lo.z = fminf(lo.z, __shfl_xor_sync(kFull, lo.z, o));
+        hi.x = fmaxf(hi.x, __shfl_xor_sync(kFull, hi.x, o));
+        hi.y = fmaxf(hi.y, __shfl_xor_sync(kFull, hi.y, o));
+        hi.z = fmaxf(hi.z, __shfl_xor_sync(kFull, hi.z, o));
+    }
+    const float k_take = theta2 * kBoxLo, k_open = theta2 * kBoxHi;
+    const int s = sg.seg;
+    const int off = (int)__ldg(L.seg_off + s);
+    const int seg_n = (int)__ldg(L.seg_off + s + 1) - off;
+    int32_t* list = fr.list + (size_t)sgi * kSuperCap;
+    int32_t* src = fr.src + (size_t)sgi * kSuperSrcCap;
+    int n_take = 0, n_src = 0, n_front = 0;
+    bool ok = true;
+    if (seg_n >= 2) {
+        int top = 1;
+        if (lane == 0) stk[0] = off - s;
+        __syncwarp();
+        int budget = seg_n - 1;
+        while (top > 0) {
+            const int b = top < 32 ? top : 32;
+            budget -= b;
+            if (budget < 0) {
+                if (lane == 0) atomicOr(status, GCS_DEV_TREE_MALFORMED);
+                ok = false;
+                break;
+            }
+            top -= b;
+            int node = -1, cls = kClassNone, code_a = 0, code_b = kWalkSkipTag;
+            if (lane < b) {
+                node = stk[top + lane];
+                const float4* np = reinterpret_cast<const float4*>(wn + node);
+                const float4 a = __ldg(np);
+                const int4 k = __ldg(reinterpret_cast<const int4*>(np + 1));
+                code_a = k.y;
+                code_b = k.z;
+                cls = box_class(a, __int_as_float(k.x), lo, hi, eps2, k_take, k_open);
+            }
+            __syncwarp();
+            const uint32_t bt = __ballot_sync(kFull, cls == kClassTake);
+            const uint32_t bm = __ballot_sync(kFull, cls == kClassMixed);
+            int n_push = 0, n_s = 0;
+            if (cls == kClassOpen && code_b != kWalkSkipTag) {
+                if (code_b >= kWalkBucketTag) {
+                    n_s = code_b - kWalkBucketTag;
+                } else {
+                    n_push = (code_a >= 0) + (code_b >= 0);
+                    n_s = (code_a < 0) + (code_b < 0);
+                }
+            }
+            const uint32_t both = ((uint32_t)n_push << 16) | (uint32_t)n_s;
+            const uint32_t excl = warp_exclusive_scan(both, lane);
+            const uint32_t total = __shfl_sync(kFull, excl + both, 31);
+            const int push_total = (int)(total >> 16), src_total = (int)(total & 0xFFFFu);
+            if (n_take + n_front + __popc(bt) + __popc(bm) > kSuperCap || n_src + src_total > kSuperSrcCap ||
+                top + push_total > kFrontStack) {
+                ok = false;
+                break;
+            }
+            if (cls == kClassTake) list[n_take + __popc(bt & lt)] = node;
+            if (cls == kClassMixed) list[kSuperCap - 1 - (n_front + __popc(bm & lt))] = node;
+            n_take += __popc(bt);
+            n_front += __popc(bm);
+            {
+                int at = top + (int)(excl >> 16);
+                if (n_push > 0) {
+                    if (code_a >= 0) stk[at++] = code_a;
+                    if (code_b >= 0) stk[at++] = code_b;
+                }
+                int sat = n_src + (int)(excl & 0xFFFFu);
+                if (n_s > 0) {
+                    if (code_b >= kWalkBucketTag) {
+                        for (int r = 0; r < n_s; ++r) src[sat + r] = code_a + r;
+                    } else {
+                        if (code_a < 0) src[sat++] = ~code_a;
+                        if (code_b < 0) src[sat++] = ~code_b;
+                    }
+                }
+            }
+            top += push_total;
+            n_src += src_total;
+            __syncwarp();
+        }
+    }
+    if (lane == 0) fr.meta[sgi] = make_int4(n_take, n_src, n_front, ok ? 1 : 0);
+}
+
 template <int H, int T>
 constexpr size_t smem_bytes() {
     return sizeof(WarpSmem<H, T>) * kWalkWarps;
@@ -780,7 +965,7 @@ template <int H, int T>
 static void launch_ht(const Layout& L, const WalkParams& q, const float4* pos, const WalkNode* wn,
                       const WalkGroup* groups, int n_groups, float4* acc, uint32_t* queue, uint32_t* status,
                       unsigned long long* counts, int2* gstack, int cap, unsigned g, cudaStream_t st,
-                      const WalkEpilogue& ep) {
+                      const WalkEpilogue& ep, const WalkFrontier& fr) {
     using Entry = typename EntryOf<T>::type;
     Entry* gs = reinterpret_cast<Entry*>(gstack);
     const size_t sm = smem_bytes<H, T>();
@@ -788,20 +973,20 @@ static void launch_ht(const Layout& L, const WalkParams& q, const float4* pos, c
         if (q.with_potential) {
             configure<H, T, true, true>();
             walk_kernel<H, T, true, true><<<g, kWalkThreads, sm, st>>>(L, q, pos, wn, groups, n_groups, acc, queue,
-                                                                       status, counts, gs, cap, ep);
+                                                                       status, counts, gs, cap, ep, fr);
         } else {
             configure<H, T, false, true>();
             walk_kernel<H, T, false, true><<<g, kWalkThreads, sm, st>>>(L, q, pos, wn, groups, n_groups, acc, queue,
-                                                                        status, counts, gs, cap, ep);
+                                                                        status, counts, gs, cap, ep, fr);
         }
     } else if (q.with_potential) {
         configure<H, T, true, false>();
         walk_kernel<H, T, true, false><<<g, kWalkThreads, sm, st>>>(L, q, pos, wn, groups, n_groups, acc, queue,
-                                                                    status, nullptr, gs, cap, ep);
+                                                                    status, nullptr, gs, cap, ep, fr);
     } else {
         configure<H, T, false, false>();
         walk_kernel<H, T, false, false><<<g, kWalkThreads, sm, st>>>(L, q, pos, wn, groups, n_groups, acc, queue,
-                                                                     status, nullptr, gs, cap, ep);
+                                                                     status, nullptr, gs, cap, ep, fr);
     }
 }
 
@@ -809,8 +994,15 @@ void launch_walk(const Layout& L, const WalkParams& wp, const float4* pos,
                  const WalkNode* wn, const WalkGroup* groups, int n_groups, int targets_per_lane, float4* acc,
                  uint32_t* queue, uint32_t* status, int blocks_per_sm, int sm_count,
                  unsigned long long* counts, int2* gstack, size_t gstack_entries, cudaStream_t st,
-                 const WalkEpilogue& ep) {
+                 const WalkEpilogue& ep, const WalkFrontier& fr_in) {
     if (n_groups <= 0) return;
+    WalkFrontier fr = fr_in;
+    if (fr.supers && fr.n_supers > 0 && fr.list && fr.src && fr.meta) {
+        const unsigned fb = (unsigned)((fr.n_supers + kFrontWarps - 1) / kFrontWarps);
+        frontier_kernel<<<fb, kFrontWarps * 32, 0, st>>>(L, pos, wn, fr, wp.eps2, wp.theta2, status);
+    } else {
+        fr.meta = nullptr;  // every group walks from its root
+    }
     WalkParams q = wp;
     if (q.batch < 1) q.batch = 1;
     if (q.batch > kWalkMaxBatch) q.batch = kWalkMaxBatch;
@@ -834,13 +1026,13 @@ void launch_walk(const Layout& L, const WalkParams& wp, const float4* pos,
     const int cap = (int)(std::min<size_t>(units, (size_t)1 << 24) / (size_t)T);
     if (T == 2) {
         if (q.batch > 32)
-            launch_ht<2, 2>(L, q, pos, wn, groups, n_groups, acc, queue, status, counts, gstack, cap, g, st, ep);
+            launch_ht<2, 2>(L, q, pos, wn, groups, n_groups, acc, queue, status, counts, gstack, cap, g, st, ep, fr);
         else
-            launch_ht<1, 2>(L, q, pos, wn, groups, n_groups, acc, queue, status, counts, gstack, cap, g, st, ep);
+            launch_ht<1, 2>(L, q, pos, wn, groups, n_groups, acc, queue, status, counts, gstack, cap, g, st, ep, fr);
     } else if (q.batch > 32) {
-        launch_ht<2, 1>(L, q, pos, wn, groups, n_groups, acc, queue, status, counts, gstack, cap, g, st, ep);
+        launch_ht<2, 1>(L, q, pos, wn, groups, n_groups, acc, queue, status, counts, gstack, cap, g, st, ep, fr);
     } else {
-        launch_ht<1, 1>(L, q, pos, wn, groups, n_groups, acc, queue, status, counts, gstack, cap, g, st, ep);
+        launch_ht<1, 1>(L, q, pos, wn, groups, n_groups, acc, queue, status, counts, gstack, cap, g, st, ep, fr);
     }
 }
 

@@ -58,6 +58,8 @@ struct gcs_server {
     cudaStream_t stream = nullptr;
     cudaEvent_t step_done[2] = {nullptr, nullptr};
     int64_t ticks = 0;
+    int64_t particle_steps = 0;  // progress counters (gcs_server_progress)
+    int64_t peak_scenarios = 0, peak_particles = 0;
     gcs_params p;
     int64_t capacity = 0;
     int32_t max_segments = 0;
@@ -242,6 +244,9 @@ int gcs_server_tick(gcs_server* s, int64_t out[4]) {
         }
         int rc = gcs_step(s->ctx, &s->p);
         if (rc) return fail(s, rc, "step");
+        s->particle_steps += particles;
+        s->peak_scenarios = std::max<int64_t>(s->peak_scenarios, (int64_t)s->resident.size());
+        s->peak_particles = std::max(s->peak_particles, particles);
         if (cudaEventRecord(ev, s->stream) != cudaSuccess) {
             cudaGetLastError();
             return fail(s, GCS_ERR_CUDA, "step event");
@@ -309,6 +314,15 @@ int gcs_server_counts(const gcs_server* s, int64_t out[3]) {
     out[0] = (int64_t)s->queued.size();
     out[1] = (int64_t)s->resident.size();
     out[2] = (int64_t)s->finished.size();
+    return GCS_OK;
+}
+
+int gcs_server_progress(const gcs_server* s, int64_t out[4]) {
+    if (!s || !out) return GCS_ERR_ARG;
+    out[0] = s->particle_steps;
+    out[1] = s->ticks;
+    out[2] = s->peak_scenarios;
+    out[3] = s->peak_particles;
     return GCS_OK;
 }
 

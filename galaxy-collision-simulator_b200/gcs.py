@@ -123,6 +123,7 @@ def lib() -> C.CDLL:
         "gcs_count_interactions": (C.c_int, [P, C.POINTER(Params), C.POINTER(C.c_uint64)]),
         "gcs_autotune": (C.c_int, [P, C.POINTER(Params), C.POINTER(C.c_double)]),
         "gcs_set_group_width": (C.c_int, [P, i32]),
+        "gcs_set_walk_frontier": (C.c_int, [P, i32]),
         "gcs_group_width": (i32, [P]),
         "gcs_sort_pairs_static": (C.c_int, [P, P, P, P, i64, P, P]),
         "gcs_set_graphs": (C.c_int, [P, i32]),
@@ -158,6 +159,7 @@ def lib() -> C.CDLL:
         "gcs_server_submit": (C.c_int, [P, u64, P, i64, i32]),
         "gcs_server_tick": (C.c_int, [P, C.POINTER(i64)]),
         "gcs_server_counts": (C.c_int, [P, C.POINTER(i64)]),
+        "gcs_server_progress": (C.c_int, [P, C.POINTER(i64)]),
         "gcs_server_pop": (C.c_int, [P, C.POINTER(ServerResult), P, i64]),
         "gcs_dropin_set_params": (C.c_int, [C.POINTER(Params)]),
         "gcs_dropin_context": (P, []),
@@ -373,6 +375,10 @@ class Context:
     def set_group_width(self, w: int) -> None:
         self.check(self.L.gcs_set_group_width(self._h, w))
 
+    def set_walk_frontier(self, enable: bool) -> None:
+        """Super-group frontier pass before the walk (on by default)."""
+        self.check(self.L.gcs_set_walk_frontier(self._h, int(bool(enable))))
+
     def count_interactions(self, p: Params, warp_evals: bool = False):
         """(monopole terms, particle terms)[, warp node evals, warp source evals,
         pop rounds, stack spills, evals opened by all lanes, evals accepted by all]."""
@@ -515,6 +521,12 @@ class Server:
     def counts(self) -> tuple:
         out = (C.c_int64 * 3)()
         self.check(self.L.gcs_server_counts(self._h, out))
+        return tuple(int(x) for x in out)
+
+    def progress(self) -> tuple:
+        """(particle-steps advanced, steps, peak resident scenarios, peak resident particles)."""
+        out = (C.c_int64 * 4)()
+        self.check(self.L.gcs_server_progress(self._h, out))
         return tuple(int(x) for x in out)
 
     def pop(self, with_stars: bool = True):

@@ -117,6 +117,16 @@ int32_t gcs_num_segments(const gcs_ctx* ctx);
  * its own walk's); speed does. */
 int gcs_set_group_width(gcs_ctx* ctx, int32_t width);
 int32_t gcs_group_width(const gcs_ctx* ctx);
+/* Walk frontiers (enable = 1, the default; no counterpart in the reference,
+ * whose walk starts every target at the root, cuda_engine.cu:100-107): before
+ * the walk, one pass per super-group of about 256 consecutive targets decides
+ * the top of the tree against the super-group's bounding box - nodes every
+ * one of its targets accepts, nodes every one opens - and each walk group
+ * evaluates the accepted nodes for all its targets and starts its own walk
+ * at the undecided nodes.  With enable = 0 every group walks from its
+ * segment's root.  Both give every target exactly its own walk's terms; only
+ * the order of the FP32 sums differs. */
+int gcs_set_walk_frontier(gcs_ctx* ctx, int32_t enable);
 
 /* ---- one scenario across devices -----------------------------------------
  * Every rank of a multi-GPU job holds the whole scenario and runs the same
@@ -472,6 +482,11 @@ int gcs_server_submit(gcs_server* srv, uint64_t id, const Star* stars, int64_t n
 int gcs_server_tick(gcs_server* srv, int64_t out[4]);
 /* out = {queued, resident, finished and not yet popped}. */
 int gcs_server_counts(const gcs_server* srv, int64_t out[3]);
+/* Progress since creation: out[0] particle-steps advanced (the resident
+ * particles of every tick's step, queued steps included), out[1] steps
+ * (ticks that stepped), out[2] peak resident scenarios, out[3] peak resident
+ * particles. */
+int gcs_server_progress(const gcs_server* srv, int64_t out[4]);
 /* Pop the oldest finished scenario: returns 1 and fills info (and host, if
  * not NULL, with its n final Stars), 0 if none has finished. */
 int gcs_server_pop(gcs_server* srv, gcs_server_result* info, Star* host, int64_t host_capacity);

@@ -187,12 +187,16 @@ void gcs_oracle_aggregate(int n, const float* xyzm, BvhNodeTraverse* nodes, floa
             r.hi[a] = fmaxf(ch[0].hi[a], ch[1].hi[a]);
         }
         const float w = fmaxf(r.hi[0] - r.lo[0], fmaxf(r.hi[1] - r.lo[1], r.hi[2] - r.lo[2]));
+        /* particles in the node: its range [min(v, j), max(v, j)] */
+        const int re = nodes[v].range_end;
+        const int count = (re > v ? re - v : v - re) + 1;
+        const int big = com_fp64 && count >= GCS_ORACLE_COM_FP64_MIN;
         r.m = ch[0].m + ch[1].m;
         r.md = ch[0].md + ch[1].md;
         for (int a = 0; a < 3; ++a) r.mx[a] = ch[0].mx[a] + ch[1].mx[a];
         for (int a = 0; a < 3; ++a) {
             if (r.m > 0.0f) {
-                if (com_fp64) r.com[a] = (float)(r.mx[a] / r.md);
+                if (big) r.com[a] = (float)(r.mx[a] / r.md);
                 else r.com[a] = fmaf(ch[0].com[a], ch[0].m, ch[1].com[a] * ch[1].m) / r.m;
             } else {
                 r.com[a] = (r.lo[a] + r.hi[a]) * 0.5f;
@@ -200,6 +204,12 @@ void gcs_oracle_aggregate(int n, const float* xyzm, BvhNodeTraverse* nodes, floa
             }
         }
         if (!(r.m > 0.0f)) r.md = 0.0;
+        if (!big && r.m > 0.0f) {
+            /* a node below the FP64 size hands its parent the exact double
+             * product of its FP32 mass and centre of mass */
+            for (int a = 0; a < 3; ++a) r.mx[a] = (double)r.m * (double)r.com[a];
+            r.md = (double)r.m;
+        }
         agg[v] = r;
         nodes[v].com_x = r.com[0];
         nodes[v].com_y = r.com[1];

@@ -47,7 +47,11 @@ void gcs_oracle_build(const uint64_t* keys, int n, int node_base, int leaf_base,
 /* karras_bvh.cuh:175-225 over one segment: fills com/mass/width of `nodes`
  * (n-1 entries, children already set, numbering as in gcs_oracle_build with
  * node_base 0 and leaf_base n-1) and box (6 floats per node).  com_fp64
- * selects FP64 mass-weighted sums instead of the FP32 pairwise formula. */
+ * selects, for nodes of at least GCS_ORACLE_COM_FP64_MIN particles (the top
+ * of the tree), FP64 mass-weighted sums instead of the FP32 pairwise formula;
+ * a child below that size (or a particle) enters those sums as the exact
+ * double product of its FP32 mass and centre of mass (or position). */
+#define GCS_ORACLE_COM_FP64_MIN 1024
 void gcs_oracle_aggregate(int n, const float* xyzm, BvhNodeTraverse* nodes, float* box,
                           int com_fp64);
 /* cuda_engine.cu:91-161 with theta and leaf size L, for every particle of

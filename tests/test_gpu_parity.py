@@ -195,6 +195,32 @@ def test_wide_groups_match_oracle(gcs_mod, oracle_mod, stars, width, batch, thet
         assert ctx.device_status() == 0
 
 
+@pytest.mark.parametrize("width,theta,leaf", [(32, 0.5, 4), (16, 0.5, 1), (64, 0.5, 8), (32, 0.7, 32),
+                                               (48, 1.0, 1), (32, 0.3, 2)])
+def test_walk_frontier_keeps_every_targets_terms(gcs_mod, oracle_mod, width, theta, leaf):
+    """The super-group frontier pass (on by default) and the walk from the
+    root (frontiers off) give every target exactly the oracle's terms: the
+    same monopole and particle counts, accelerations and potentials within
+    the walk tolerance; several super-groups of uneven size per segment."""
+    gcs = gcs_mod
+    st = small_collision(4096, 1024, 512, seed=31)  # 11,264 particles
+    with _ctx(gcs, st) as ctx:
+        ctx.set_group_width(width)
+        p = _params(gcs, theta=theta, leaf_size=leaf, walk_batch=64, with_potential=1)
+        ctx.run_stages(p, gcs.STAGE_BOUNDS, gcs.STAGE_AGGREGATE)
+        sp = ctx.read(gcs.BUF_POS)
+        ref, cnt = oracle_mod.walk(sp, ctx.read(gcs.BUF_NODES), p.G, p.epsilon_sq, theta, leaf, counts=True)
+        want = (int(cnt[:, 0].sum()), int(cnt[:, 1].sum()))
+        for frontier in (True, False):
+            ctx.set_walk_frontier(frontier)
+            ctx.run_stages(p, gcs.STAGE_WALK, gcs.STAGE_WALK)
+            acc = ctx.read(gcs.BUF_ACCEL)
+            _assert_acc(acc[:, :3], ref[:, :3], "frontier=%s width=%d theta=%s L=%d" % (frontier, width, theta, leaf))
+            np.testing.assert_allclose(acc[:, 3], ref[:, 3], rtol=1e-5)
+            assert ctx.count_interactions(p) == want, frontier
+        assert ctx.device_status() == 0
+
+
 def test_wide_groups_in_segments(gcs_mod, stars):
     """Two targets per lane over uneven segments (groups never straddle a
     segment): each segment's accelerations equal the segment walked alone."""
