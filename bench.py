@@ -426,23 +426,36 @@ def accuracy(gcs, ctx, p, stars, n_sub=65536, seed=0):
     out = {"subset": int(len(tg)), "theta": p.theta, "leaf_size": p.leaf_size, "engine": stats(acc)}
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle  # noqa: PLC0415
-    if oracle.ref_lib("ref_cuda") is not None:
-        pos, _ = gcs.pos_vel_from_stars(stars)
-        lo, hi = float(pos[:, :3].min()), float(pos[:, :3].max())
+    has_ref = oracle.ref_lib("ref_cuda") is not None
+    pos, _ = gcs.pos_vel_from_stars(stars)
+    lo, hi = float(pos[:, :3].min()), float(pos[:, :3].max())
+
+    def ref_stats(theta):
         ref = oracle.RefCuda(n)
         try:
-            ref.set_theta(p.theta)
+            ref.set_theta(theta)
             ref.upload(stars)
             ref.step_device(p.G, p.epsilon_sq, 0.0, lo, hi)
             same_order = bool(np.array_equal(ref.read(0), keys))
             racc = ref.read(4).astype(np.float64)
         finally:
             ref.close()
-        if same_order:  # identical keys -> identical stable permutation
-            out["reference_gpu"] = stats(racc)
-            out["reference_gpu"]["leaf_size"] = 1
-        else:
-            out["reference_gpu"] = {"unavailable": "sorted orders differ"}
+        if not same_order:  # identical keys -> identical stable permutation
+            return {"unavailable": "sorted orders differ"}
+        r = stats(racc)
+        r["leaf_size"] = 1
+        return r
+
+    if has_ref:
+        out["reference_gpu"] = ref_stats(p.theta)
+    # the recipe's other theta (0.7): engine and reference on the same snapshot
+    q = gcs.Params.from_buffer_copy(p)
+    q.theta = 0.7
+    ctx.upload(stars)
+    ctx.compute_accels(q)
+    out["theta_0.7"] = {"engine": stats(ctx.read(gcs.BUF_ACCEL)[:, :3].astype(np.float64))}
+    if has_ref:
+        out["theta_0.7"]["reference_gpu"] = ref_stats(0.7)
     return out
 
 

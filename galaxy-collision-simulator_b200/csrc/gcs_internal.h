@@ -209,7 +209,7 @@ constexpr int kWalkBlockWarps = 8;  // warps per walk block
 // invalid and its groups walk from the root.
 constexpr int kSuperTargets = 256;
 constexpr int kSuperCap = 2048;     // take nodes (from the front) + frontier nodes (from the back)
-constexpr int kSuperSrcCap = 64;    // particle sources of a super-group
+constexpr int kSuperSrcCap = 256;   // particle sources of a super-group
 // Targets [start, start + count) of segment seg (a run of whole groups).
 struct SuperGroup {
     int32_t start;

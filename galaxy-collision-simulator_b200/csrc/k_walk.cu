@@ -410,14 +410,15 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                     WC.w_node += (uint32_t)fm.x;
                     WC.all_take += (uint32_t)fm.x;
                 }
-                if (fm.y > 0) {
-                    const int32_t* sl = fr.src + (size_t)grp.super * kSuperSrcCap;
-                    for (int e = lane; e < fm.y; e += 32) {
-                        W.srcp[e] = __ldg(sl + e);
+                const int32_t* sl = fr.src + (size_t)grp.super * kSuperSrcCap;
+                for (int base = 0; base < fm.y; base += kSrcCap) {
+                    const int cnt = min(kSrcCap, fm.y - base);
+                    for (int e = lane; e < cnt; e += 32) {
+                        W.srcp[e] = __ldg(sl + base + e);
 #pragma unroll
                         for (int t = 0; t < T; ++t) W.srcm[t][e] = live[t];
                     }
-                    flush_sources<H, T, kPot, kCount>(W, fm.y, lane, lane_bit, pos, G, X, e2, leaf_thr, A, WC);
+                    flush_sources<H, T, kPot, kCount>(W, cnt, lane, lane_bit, pos, G, X, e2, leaf_thr, A, WC);
                 }
                 // frontier entries [kSuperCap - n_front, kSuperCap): what the
                 // shared stack cannot hold goes to the global bottom
