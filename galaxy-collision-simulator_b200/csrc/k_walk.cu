@@ -779,18 +779,18 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
 }
 
 // Frontier pass (WalkFrontier, gcs_internal.h): one warp per super-group
-// walks the tree against the super-group's bounding box, 32 nodes per round
-// (lane k classifies node k with box_class).  Certified take nodes are
-// appended to the take list, undecided ones to the frontier, and nodes every
-// target opens contribute their internal children to the stack and their
-// particles (leaf children, or the whole range of a small node) to the
-// source list, in the order the group walk would use them.  Lists grow at
-// offsets from warp ballots and scans; a list or stack that would overflow,
-// or more pops than the segment has internal nodes, marks the super-group
-// invalid (its groups then walk from the root), so nothing is written out of
-// bounds.
+// walks the tree against the super-group's bounding box, up to 64 nodes per
+// round (lane k classifies nodes k and k + 32 with box_class).  Certified
+// take nodes are appended to the take list, undecided ones to the frontier,
+// and nodes every target opens contribute their internal children to the
+// stack and their particles (leaf children, or the whole range of a small
+// node) to the source list.  Lists grow at offsets from warp ballots and
+// scans; a list or stack that would overflow, or more pops than the segment
+// has internal nodes, marks the super-group invalid (its groups then walk
+// from the root), so nothing is written out of bounds.
 constexpr int kFrontWarps = 8;
 constexpr int kFrontStack = 1024;
+constexpr int kFrontSlots = 2;  // nodes per lane per round
 
 __global__ void __launch_bounds__(kFrontWarps * 32)
 frontier_kernel(Layout L, const float4* __restrict__ pos, const WalkNode* __restrict__ wn, WalkFrontier fr,
@@ -831,7 +831,7 @@ frontier_kernel(Layout L, const float4* __restrict__ pos, const WalkNode* __rest
         __syncwarp();
         int budget = seg_n - 1;
         while (top > 0) {
-            const int b = top < 32 ? top : 32;
+            const int b = top < 32 * kFrontSlots ? top : 32 * kFrontSlots;
             budget -= b;
             if (budget < 0) {
                 if (lane == 0) atomicOr(status, GCS_DEV_TREE_MALFORMED);
@@ -839,57 +839,80 @@ frontier_kernel(Layout L, const float4* __restrict__ pos, const WalkNode* __rest
                 break;
             }
             top -= b;
-            int node = -1, cls = kClassNone, code_a = 0, code_b = kWalkSkipTag;
-            if (lane < b) {
-                node = stk[top + lane];
-                const float4* np = reinterpret_cast<const float4*>(wn + node);
-                const float4 a = __ldg(np);
-                const int4 k = __ldg(reinterpret_cast<const int4*>(np + 1));
-                code_a = k.y;
-                code_b = k.z;
-                cls = box_class(a, __int_as_float(k.x), lo, hi, eps2, k_take, k_open);
-            }
-            __syncwarp();
-            const uint32_t bt = __ballot_sync(kFull, cls == kClassTake);
-            const uint32_t bm = __ballot_sync(kFull, cls == kClassMixed);
-            int n_push = 0, n_s = 0;
-            if (cls == kClassOpen && code_b != kWalkSkipTag) {
-                if (code_b >= kWalkBucketTag) {
-                    n_s = code_b - kWalkBucketTag;
-                } else {
-                    n_push = (code_a >= 0) + (code_b >= 0);
-                    n_s = (code_a < 0) + (code_b < 0);
+            int node[kFrontSlots], cls[kFrontSlots], code_a[kFrontSlots], code_b[kFrontSlots];
+#pragma unroll
+            for (int h = 0; h < kFrontSlots; ++h) {
+                node[h] = -1;
+                cls[h] = kClassNone;
+                code_a[h] = 0;
+                code_b[h] = kWalkSkipTag;
+                if (lane + 32 * h < b) {
+                    node[h] = stk[top + lane + 32 * h];
+                    const float4* np = reinterpret_cast<const float4*>(wn + node[h]);
+                    const float4 a = __ldg(np);
+                    const int4 k = __ldg(reinterpret_cast<const int4*>(np + 1));
+                    code_a[h] = k.y;
+                    code_b[h] = k.z;
+                    cls[h] = box_class(a, __int_as_float(k.x), lo, hi, eps2, k_take, k_open);
                 }
             }
-            const uint32_t both = ((uint32_t)n_push << 16) | (uint32_t)n_s;
+            __syncwarp();
+            uint32_t bt[kFrontSlots], bm[kFrontSlots];
+            int add_take = 0, add_front = 0, lane_push = 0, lane_src = 0;
+            int n_push[kFrontSlots], n_s[kFrontSlots];
+#pragma unroll
+            for (int h = 0; h < kFrontSlots; ++h) {
+                bt[h] = __ballot_sync(kFull, cls[h] == kClassTake);
+                bm[h] = __ballot_sync(kFull, cls[h] == kClassMixed);
+                add_take += __popc(bt[h]);
+                add_front += __popc(bm[h]);
+                n_push[h] = 0;
+                n_s[h] = 0;
+                if (cls[h] == kClassOpen && code_b[h] != kWalkSkipTag) {
+                    if (code_b[h] >= kWalkBucketTag) {
+                        n_s[h] = code_b[h] - kWalkBucketTag;
+                    } else {
+                        n_push[h] = (code_a[h] >= 0) + (code_b[h] >= 0);
+                        n_s[h] = (code_a[h] < 0) + (code_b[h] < 0);
+                    }
+                }
+                lane_push += n_push[h];
+                lane_src += n_s[h];
+            }
+            const uint32_t both = ((uint32_t)lane_push << 16) | (uint32_t)lane_src;
             const uint32_t excl = warp_exclusive_scan(both, lane);
             const uint32_t total = __shfl_sync(kFull, excl + both, 31);
             const int push_total = (int)(total >> 16), src_total = (int)(total & 0xFFFFu);
-            if (n_take + n_front + __popc(bt) + __popc(bm) > kSuperCap || n_src + src_total > kSuperSrcCap ||
+            if (n_take + n_front + add_take + add_front > kSuperCap || n_src + src_total > kSuperSrcCap ||
                 top + push_total > kFrontStack) {
                 ok = false;
                 break;
             }
-            if (cls == kClassTake) list[n_take + __popc(bt & lt)] = node;
-            if (cls == kClassMixed) list[kSuperCap - 1 - (n_front + __popc(bm & lt))] = node;
-            n_take += __popc(bt);
-            n_front += __popc(bm);
-            {
-                int at = top + (int)(excl >> 16);
-                if (n_push > 0) {
-                    if (code_a >= 0) stk[at++] = code_a;
-                    if (code_b >= 0) stk[at++] = code_b;
+            int take_before = 0, front_before = 0;
+            int at = top + (int)(excl >> 16), sat = n_src + (int)(excl & 0xFFFFu);
+#pragma unroll
+            for (int h = 0; h < kFrontSlots; ++h) {
+                if (cls[h] == kClassTake) list[n_take + take_before + __popc(bt[h] & lt)] = node[h];
+                if (cls[h] == kClassMixed)
+                    list[kSuperCap - 1 - (n_front + front_before + __popc(bm[h] & lt))] = node[h];
+                take_before += __popc(bt[h]);
+                front_before += __popc(bm[h]);
+                if (n_push[h] > 0) {
+                    if (code_a[h] >= 0) stk[at++] = code_a[h];
+                    if (code_b[h] >= 0) stk[at++] = code_b[h];
                 }
-                int sat = n_src + (int)(excl & 0xFFFFu);
-                if (n_s > 0) {
-                    if (code_b >= kWalkBucketTag) {
-                        for (int r = 0; r < n_s; ++r) src[sat + r] = code_a + r;
+                if (n_s[h] > 0) {
+                    if (code_b[h] >= kWalkBucketTag) {
+                        for (int r = 0; r < n_s[h]; ++r) src[sat + r] = code_a[h] + r;
+                        sat += n_s[h];
                     } else {
-                        if (code_a < 0) src[sat++] = ~code_a;
-                        if (code_b < 0) src[sat++] = ~code_b;
+                        if (code_a[h] < 0) src[sat++] = ~code_a[h];
+                        if (code_b[h] < 0) src[sat++] = ~code_b[h];
                     }
                 }
             }
+            n_take += add_take;
+            n_front += add_front;
             top += push_total;
             n_src += src_total;
             __syncwarp();

@@ -407,7 +407,13 @@ void gcs_camera_reference(gcs_camera* cam);
  * pos), as the reference does every frame while the camera is locked on the
  * centre of mass or, in Playback mode, the frame's mean position
  * (renderer.cpp:255-256; the target from gcs_playback_centre or
- * cuda_get_center_of_mass).  GCS_ERR_ARG when target is the eye. */
+ * cuda_get_center_of_mass).  The direction is formed as d * (1 / |d|); the
+ * reference's glm::normalize multiplies by an inverse square root, so the two
+ * agree up to the last bit of rounding.  The reference also re-derives its
+ * mouse-look yaw and pitch from the new front (renderer.cpp:257-258); that
+ * interactive state has no counterpart here (a caller that keeps one uses
+ * pitch = asin(front.y), yaw = atan2(front.z, front.x)).  GCS_ERR_ARG when
+ * target is the eye. */
 int gcs_camera_look_at(gcs_camera* cam, const float target[3]);
 /* The 4x4 view and projection matrices (row-major, applied to column
  * vectors) the renderer uses for cam at width x height: glm::lookAt(pos,
