@@ -367,16 +367,20 @@ def test_edge_cases(gcs_mod, oracle_mod):
     same = st.copy()
     same["x"], same["y"], same["z"] = 1.5, 1.5, 1.5   # max == min: scale is inf, (x-min)*scale is NaN -> 0
     with _ctx(gcs, same) as ctx:
-        # FP64 sums give the exact centre of mass: every term has dx = 0
-        ctx.run_stages(_params(gcs, com_fp64=1), gcs.STAGE_BOUNDS, gcs.STAGE_WALK)
-        assert np.all(ctx.read(gcs.BUF_KEYS) == 0)
-        assert np.all(ctx.read(gcs.BUF_ACCEL)[:, :3] == 0)
-        # the reference's FP32 formula rounds the COM of unequal masses off the
-        # point by an ulp; the result must still be the oracle's
-        p = _params(gcs, com_fp64=0)
-        ctx.run_stages(p, gcs.STAGE_BOUNDS, gcs.STAGE_WALK)
-        ref = oracle_mod.walk(ctx.read(gcs.BUF_POS), ctx.read(gcs.BUF_NODES), p.G, p.epsilon_sq, p.theta, 1)
-        np.testing.assert_allclose(ctx.read(gcs.BUF_ACCEL)[:, :3], ref[:, :3], rtol=1e-5)
+        # the FP32 pairwise formula (every node here is below the FP64 size)
+        # rounds the COM of unequal masses off the point by an ulp: with
+        # either setting the result must be the oracle's
+        for com in (1, 0):
+            p = _params(gcs, com_fp64=com)
+            ctx.run_stages(p, gcs.STAGE_BOUNDS, gcs.STAGE_WALK)
+            assert np.all(ctx.read(gcs.BUF_KEYS) == 0)
+            nodes = ctx.read(gcs.BUF_NODES)
+            ref_nodes, _ = oracle_mod.aggregate(ctx.read(gcs.BUF_POS), nodes["child_left"], nodes["child_right"],
+                                                nodes["range_end"], com_fp64=bool(com))
+            for f in ("com_x", "com_y", "com_z", "mass"):
+                np.testing.assert_array_equal(nodes[f], ref_nodes[f])
+            ref = oracle_mod.walk(ctx.read(gcs.BUF_POS), nodes, p.G, p.epsilon_sq, p.theta, 1)
+            np.testing.assert_allclose(ctx.read(gcs.BUF_ACCEL)[:, :3], ref[:, :3], rtol=1e-5)
         assert ctx.device_status() == 0
     # two particles
     with _ctx(gcs, st[:2]) as ctx:
