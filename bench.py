@@ -78,7 +78,8 @@ def parse():
     ap.add_argument("--batched-steps", type=int, default=10)
     ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--served-requests", type=int, default=240)
-    ap.add_argument("--served-window", type=float, default=10.0, help="seconds served per load and mode")
+    ap.add_argument("--served-window", type=float, default=10.0,
+                    help="seconds served per load and mode (<= 0: until every request has finished)")
     ap.add_argument("--served-loads", type=lambda v: [float(x) for x in v.split(",")], default=[0.5, 1.0, 1.5, 2.0],
                     help="offered loads as multiples of the one-at-a-time capacity")
     return ap.parse_args()
@@ -710,7 +711,8 @@ def batched_bench(gcs, torch, args):
 
 
 def _serve_window(gcs, p, reqs, stars, max_segments, budget, window_s):
-    """Drive a server for `window_s` seconds with requests arriving at their
+    """Drive a server for `window_s` seconds (window_s <= 0: until every
+    request has arrived and finished) with requests arriving at their
     wall-clock times: returns per-completed-request latencies (ms), the
     particle-steps the server advanced over the window, its wall time (to the
     last step's completion) and the peak residency."""
@@ -721,7 +723,7 @@ def _serve_window(gcs, p, reqs, stars, max_segments, budget, window_s):
         i, R = 0, len(reqs)
         while True:
             now = time.perf_counter() - t0
-            if now >= window_s:
+            if (window_s > 0 and now >= window_s) or (window_s <= 0 and len(lat) == R):
                 break
             while i < R and reqs[i].arrival_s <= now:
                 srv.submit(i, stars[i], reqs[i].steps)

@@ -296,27 +296,31 @@ int upload_groups(gcs_ctx* c) {
     std::vector<SuperGroup> supers;
     groups.reserve((size_t)(c->n / c->group_width + c->nseg + 1));
     const int64_t rf = range_first(c), rl = rf + range_count(c);
+    // Super-groups are aligned to the segment start and always cover all of
+    // their targets, also where a step range cuts one: its box, and so its
+    // frontier and every group's sums, are then the same in each slice of a
+    // scenario stepped across devices as in the whole scenario.
     const int per = groups_per_super(c->group_width);
+    const int64_t span = (int64_t)per * c->group_width;  // targets of a full super-group
     for (int s = 0; s < c->nseg; ++s) {
         const int64_t a = c->h_seg_off[s], e = c->h_seg_off[s + 1];
-        int in_super = per;  // groups in the current super-group (a segment starts a new one)
+        int64_t cur = -1;  // first target of the current super-group
         for (int64_t g = a; g < e; g += c->group_width) {
             if (g < rf || g >= rl) continue;  // outside this context's step range
             WalkGroup w;
             w.start = (int32_t)g;
             w.count = (int32_t)std::min<int64_t>(c->group_width, e - g);
             w.seg = s;
-            if (in_super == per) {
+            const int64_t sg_first = a + (g - a) / span * span;
+            if (sg_first != cur) {
                 SuperGroup sg;
-                sg.start = w.start;
-                sg.count = 0;
+                sg.start = (int32_t)sg_first;
+                sg.count = (int32_t)std::min<int64_t>(span, e - sg_first);
                 sg.seg = s;
                 sg.pad = 0;
                 supers.push_back(sg);
-                in_super = 0;
+                cur = sg_first;
             }
-            supers.back().count += w.count;
-            ++in_super;
             w.super = (int32_t)supers.size() - 1;
             groups.push_back(w);
         }
