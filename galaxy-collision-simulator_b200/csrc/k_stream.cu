@@ -153,23 +153,6 @@ __global__ void bounds_decode_kernel(const uint32_t* __restrict__ enc, float2* _
         out[s] = make_float2(ordered_to_float(~enc[2 * s]), ordered_to_float(enc[2 * s + 1]));
 }
 
-// Count `digit` for the valid lanes of the warp (`valid_mask`, a prefix of
-// the lanes): lanes whose digit equals their predecessor's join its run and
-// the run's first lane adds the run length.  From the second step on the
-// particles arrive nearly in Morton order, so the high digits of a warp form
-// one or two runs, where per-lane atomics on one address would serialise.
-__device__ __forceinline__ void count_digit_runs(uint32_t* h, uint32_t digit, bool valid, uint32_t valid_mask,
-                                                 int lane) {
-    const uint32_t prev = __shfl_up_sync(0xFFFFFFFFu, digit, 1);
-    const bool head = valid && (lane == 0 || digit != prev);
-    const uint32_t heads = __ballot_sync(0xFFFFFFFFu, head);
-    if (head) {
-        const uint32_t later = heads & ~((2u << lane) - 1u);  // heads after this lane (2u << 31 wraps to 0)
-        const int end = later ? __ffs(later) - 1 : 32 - __clz(valid_mask);
-        atomicAdd(h + digit, (uint32_t)(end - lane));
-    }
-}
-
 // keys[i] = 63-bit Morton code of particle i in its segment's cube; idx[i] = i
 // (karras_bvh.cuh:34-41).  The radix sort's global digit histograms (8 key
 // digits, plus the segment-id digits when there is more than one segment)
@@ -183,38 +166,27 @@ __global__ void encode_kernel(Layout L, const float4* __restrict__ pos, int boun
     const int passes = kKeyPasses + n_seg_passes;
     for (int t = threadIdx.x; t < passes * kRadix; t += blockDim.x) (&s_hist[0][0])[t] = 0;
     __syncthreads();
-    const int lane = threadIdx.x & 31;
     float lo = gmin, scale = 0.0f;
     int cur_seg = -1;
     if (bounds_mode == GCS_BOUNDS_CALLER) scale = morton_scale(gmin, gmax);
-    // whole warps iterate together (the run counting is warp-wide); lanes
-    // past the end take part without a particle
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t base = blockIdx.x * (int64_t)blockDim.x + (threadIdx.x & ~31); base < L.n; base += stride) {
-        const int64_t i = base + lane;
-        const bool valid = i < L.n;
-        const uint32_t valid_mask = __ballot_sync(0xFFFFFFFFu, valid);
-        uint64_t k = 0;
-        int seg = 0;
-        if (valid) {
-            const float4 p = __ldg(pos + i);
-            seg = (L.nseg > 1) ? __ldg(L.seg_id + i) : 0;
-            if (bounds_mode != GCS_BOUNDS_CALLER && seg != cur_seg) {
-                const float2 b = __ldg(seg_bounds + seg);
-                lo = b.x;
-                scale = morton_scale(b.x, b.y);
-                cur_seg = seg;
-            }
-            k = morton63(p.x, p.y, p.z, lo, scale);
-            keys[i] = k;
-            idx[i] = (uint32_t)i;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < L.n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const float4 p = __ldg(pos + i);
+        const int seg = (L.nseg > 1) ? __ldg(L.seg_id + i) : 0;
+        if (bounds_mode != GCS_BOUNDS_CALLER && seg != cur_seg) {
+            const float2 b = __ldg(seg_bounds + seg);
+            lo = b.x;
+            scale = morton_scale(b.x, b.y);
+            cur_seg = seg;
         }
+        const uint64_t k = morton63(p.x, p.y, p.z, lo, scale);
+        keys[i] = k;
+        idx[i] = (uint32_t)i;
 #pragma unroll
         for (int d = 0; d < kKeyPasses; ++d)
-            count_digit_runs(s_hist[d], (uint32_t)(k >> (kRadixBits * d)) & (kRadix - 1), valid, valid_mask, lane);
+            atomicAdd(&s_hist[d][(uint32_t)(k >> (kRadixBits * d)) & (kRadix - 1)], 1u);
         for (int d = 0; d < n_seg_passes; ++d)
-            count_digit_runs(s_hist[kKeyPasses + d], ((uint32_t)seg >> (kRadixBits * d)) & (kRadix - 1), valid,
-                             valid_mask, lane);
+            atomicAdd(&s_hist[kKeyPasses + d][((uint32_t)seg >> (kRadixBits * d)) & (kRadix - 1)], 1u);
     }
     __syncthreads();
     for (int t = threadIdx.x; t < passes * kRadix; t += blockDim.x) {
