@@ -779,9 +779,10 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
 }
 
 // Frontier pass (WalkFrontier, gcs_internal.h): one warp per super-group
-// walks the tree against the super-group's bounding box, up to 128 nodes per
-// round (lane k classifies nodes k, k + 32, k + 64 and k + 96 with box_class;
-// the pass is a chain of dependent rounds, so wide rounds shorten it).  Certified
+// walks the tree against the super-group's bounding box, up to 64 nodes per
+// round (lane k classifies nodes k and k + 32 with box_class).  The pass is a
+// chain of dependent rounds, about one per tree level, so wider rounds do not
+// shorten it.  Certified
 // take nodes are appended to the take list, undecided ones to the frontier,
 // and nodes every target opens contribute their internal children to the
 // stack and their particles (leaf children, or the whole range of a small
@@ -791,11 +792,9 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
 // from the root), so nothing is written out of bounds.
 constexpr int kFrontWarps = 8;
 constexpr int kFrontStack = 1024;
-constexpr int kFrontSlots = 4;  // nodes per lane per round
+constexpr int kFrontSlots = 2;  // nodes per lane per round
 
-// 4 blocks per SM: 64 registers, so one super-group per warp fits one wave
-// (4,736 resident warps) up to about 1.2M targets
-__global__ void __launch_bounds__(kFrontWarps * 32, 4)
+__global__ void __launch_bounds__(kFrontWarps * 32)
 frontier_kernel(Layout L, const float4* __restrict__ pos, const WalkNode* __restrict__ wn, WalkFrontier fr,
                 float eps2, float theta2, uint32_t* __restrict__ status) {
     __shared__ int32_t stk_all[kFrontWarps][kFrontStack];
