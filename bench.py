@@ -218,11 +218,12 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi, 200 ms"}
 
 
-def shard_slices(n, world, align=64):
+def shard_slices(n, world, align=256):
     """Slices of n sorted particles over `world` ranks for one scenario stepped
     across devices: every slice is L = ceil(n / world) rounded up to `align`
     particles long (so its bounds are walk-group starts for group widths that
-    divide `align`), the last ones cut at n.  Returns (L, [(first, count)])."""
+    divide `align`, and super-group starts - 256 targets - where the walk
+    partitions super-groups), the last ones cut at n.  Returns (L, [(first, count)])."""
     per = -(-n // world)
     length = -(-per // align) * align
     out = []
@@ -558,7 +559,7 @@ def run_sharded(args, gcs, torch, dist, rank, world, local):
     value = particles x steps / the slowest rank's time."""
     stars = gcs.collision_equal(*counts_for(args.n), seed=0)
     n = len(stars)
-    length, slices = shard_slices(n, world, 64)
+    length, slices = shard_slices(n, world, 256)
     first, count = slices[rank]
     stream = torch.cuda.current_stream()
     ctx = gcs.Context(max(n, world * length), device=local)

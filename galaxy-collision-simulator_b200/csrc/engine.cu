@@ -70,6 +70,8 @@ struct gcs_ctx {
     int4* sg_meta = nullptr;
     int n_supers = 0;
     size_t supers_cap = 0;
+    int32_t* perm = nullptr;              // walk targets in group order (full super-groups partitioned)
+    std::vector<int32_t> h_group_super;   // super-group of each walk group (host copy)
     Chunk* chunks = nullptr;
     float2* seg_bounds = nullptr;
     Star* staging = nullptr;
@@ -231,7 +233,7 @@ void free_all(gcs_ctx* c) {
     if (c->star_flags) cudaFreeHost(c->star_flags);
     void* ptrs[] = {c->pos[0], c->pos[1], c->vel[0], c->vel[1], c->acc, c->keys[0], c->keys[1],
                     c->idx[0], c->idx[1], c->tr, c->bd, c->wn, c->com64, c->leaf_parent, c->seg_off,
-                    c->seg_id, c->groups, c->supers, c->sg_list, c->sg_src, c->sg_meta, c->chunks,
+                    c->seg_id, c->groups, c->supers, c->sg_list, c->sg_src, c->sg_meta, c->perm, c->chunks,
                     c->seg_bounds, c->staging, c->pb_staging,
                     c->scratch, c->status, c->diag, c->targets, c->direct_out, c->counts,
                     c->walk_stack, c->render_acc, c->render_rgba, c->star_chunk_done};
@@ -278,18 +280,33 @@ int64_t range_count(const gcs_ctx* c) {
     return c->range_count < 0 ? c->n : std::max<int64_t>(0, std::min<int64_t>(c->range_count, c->n - f));
 }
 
-// A range boundary must be the end of the particles or the first particle
-// of a walk group (so that no group is split between ranges).
-bool range_boundary_ok(const gcs_ctx* c, int64_t b) {
-    if (b == c->n) return true;
-    for (int s = 0; s < c->nseg; ++s)
-        if (b >= c->h_seg_off[s] && b < c->h_seg_off[s + 1]) return (b - c->h_seg_off[s]) % c->group_width == 0;
-    return false;
-}
-
 // Groups per super-group for a group width: whole groups of at most
 // kSuperTargets targets (at least one group).
 int groups_per_super(int width) { return std::max(1, kSuperTargets / width); }
+
+// Bisection levels that split a full super-group into its groups (0: the
+// width does not halve kSuperTargets down to itself, targets stay in Morton
+// order).
+int split_levels(int width) {
+    int levels = 0;
+    for (int part = kSuperTargets; part > width; part >>= 1) ++levels;
+    return (kSuperTargets >> levels) == width ? levels : 0;
+}
+
+// Whether the walk takes its targets through a partition of each super-group.
+bool partitioned(const gcs_ctx* c) { return c->walk_frontier && split_levels(c->group_width) > 0; }
+
+// A range boundary must be the end of the particles or the first particle
+// of a walk group (so that no group is split between ranges) - of a
+// super-group when groups take their targets through a partition of their
+// super-group (so that no target moves between ranges).
+bool range_boundary_ok(const gcs_ctx* c, int64_t b) {
+    if (b == c->n) return true;
+    const int64_t unit = partitioned(c) ? (int64_t)groups_per_super(c->group_width) * c->group_width : c->group_width;
+    for (int s = 0; s < c->nseg; ++s)
+        if (b >= c->h_seg_off[s] && b < c->h_seg_off[s + 1]) return (b - c->h_seg_off[s]) % unit == 0;
+    return false;
+}
 
 int upload_groups(gcs_ctx* c) {
     std::vector<WalkGroup> groups;
@@ -338,6 +355,8 @@ int upload_groups(gcs_ctx* c) {
                                     cudaMemcpyHostToDevice, c->stream));
     c->n_supers = (int)supers.size();
     c->n_groups = (int)groups.size();
+    c->h_group_super.resize(groups.size());
+    for (size_t g = 0; g < groups.size(); ++g) c->h_group_super[g] = groups[g].super;
     c->h_group_start.resize(groups.size());
     for (size_t g = 0; g < groups.size(); ++g) c->h_group_start[g] = groups[g].start;
     return GCS_OK;
@@ -374,6 +393,8 @@ static int walk_stage(gcs_ctx* c, const gcs_params* p, const WalkEpilogue& ep) {
     fr.list = c->sg_list;
     fr.src = c->sg_src;
     fr.meta = c->sg_meta;
+    fr.perm = partitioned(c) ? c->perm : nullptr;
+    fr.split_levels = split_levels(c->group_width);
     launch_walk(L, wp, c->pos[c->cur], c->wn, c->groups, c->n_groups, c->group_width > 32 ? 2 : 1, c->acc,
                 scratch_at<uint32_t>(c, sl.walk_q), c->status, p->walk_blocks_per_sm, c->sm_count,
                 c->count_walk ? c->counts : nullptr, c->walk_stack, c->walk_stack_entries, st, ep, fr);
@@ -610,6 +631,7 @@ static int allocate_state(gcs_ctx* c) {
     if (!rc) rc |= dalloc(c, &c->sg_list, max_supers * (size_t)kSuperCap);
     if (!rc) rc |= dalloc(c, &c->sg_src, max_supers * (size_t)kSuperSrcCap);
     if (!rc) rc |= dalloc(c, &c->sg_meta, max_supers);
+    if (!rc) rc |= dalloc(c, &c->perm, N);
     if (!rc) rc |= dalloc(c, &c->chunks, max_chunks);
     if (!rc) rc |= dalloc(c, &c->seg_bounds, (size_t)max_segments);
     if (!rc) rc |= dalloc(c, &c->staging, N);
@@ -780,8 +802,15 @@ int32_t gcs_group_width(const gcs_ctx* c) { return c ? c->group_width : 0; }
 
 int gcs_set_walk_frontier(gcs_ctx* c, int32_t enable) {
     if (!c) return GCS_ERR_ARG;
-    if (c->walk_frontier != (enable != 0)) drop_graphs(c);
+    const bool old = c->walk_frontier;
     c->walk_frontier = enable != 0;
+    if (c->range_count >= 0 &&
+        (!range_boundary_ok(c, c->range_first) || !range_boundary_ok(c, c->range_first + c->range_count))) {
+        c->walk_frontier = old;
+        c->last_error = "walk frontiers partition super-groups that the step range would split";
+        return GCS_ERR_STATE;
+    }
+    if (old != c->walk_frontier) drop_graphs(c);
     return GCS_OK;
 }
 
@@ -1003,10 +1032,27 @@ static int step_host_overlapped(gcs_ctx* c, const gcs_params* p, Star* host) {
     const int tail_groups = (int)std::min<int64_t>(ng, 2 * resident);
     const int head_groups = ng - tail_groups;
     const int hpc = head_groups > 0 ? (head_groups + kMaxStarHeadChunks - 1) / kMaxStarHeadChunks : 1;
-    const int head_chunks = head_groups > 0 ? (head_groups + hpc - 1) / hpc : 0;
     const int tpc = (tail_groups + kMaxStarTailChunks - 1) / kMaxStarTailChunks;
-    const int tail_chunks = (tail_groups + tpc - 1) / tpc;
-    const int chunks = head_chunks + tail_chunks;
+    // chunk boundaries (group indices): large chunks over the head, small
+    // ones over the tail; with partitioned super-groups each boundary moves
+    // up to the next super-group edge, so a chunk's particles stay one range
+    std::vector<int32_t> bound;
+    bound.push_back(0);
+    const bool snap = partitioned(c);
+    auto add_bound = [&](int g) {
+        if (snap)
+            while (g < ng && g > 0 && c->h_group_super[(size_t)g] == c->h_group_super[(size_t)g - 1]) ++g;
+        if (g > bound.back()) bound.push_back(g);
+    };
+    for (int g = hpc; g < head_groups; g += hpc) add_bound(g);
+    add_bound(head_groups);
+    for (int g = head_groups + tpc; g < ng; g += tpc) add_bound(g);
+    add_bound(ng);
+    const int chunks = (int)bound.size() - 1;
+    if (chunks < 1 || chunks > kMaxStarChunks) {
+        c->last_error = "host step: chunk table out of range";
+        return GCS_ERR_STATE;
+    }
     if (++c->star_epoch == 0) c->star_epoch = 1;
     const uint32_t epoch = c->star_epoch;
     GCS_CUDA(c, cudaMemsetAsync(c->star_chunk_done, 0, sizeof(uint32_t) * (size_t)chunks, c->stream));
@@ -1017,10 +1063,8 @@ static int step_host_overlapped(gcs_ctx* c, const gcs_params* p, Star* host) {
     ep.stars = reinterpret_cast<float4*>(c->staging);
     ep.dt = p->dt;
     ep.recolor = p->recolor;
-    ep.head_groups = head_groups;
-    ep.head_per_chunk = hpc;
-    ep.head_chunks = head_chunks;
-    ep.tail_per_chunk = tpc;
+    ep.n_chunks = chunks;
+    for (int k = 0; k <= chunks; ++k) ep.chunk_bound[k] = bound[(size_t)k];
     ep.chunk_done = c->star_chunk_done;
     ep.host_flags = c->star_flags_dev;
     ep.epoch = epoch;
@@ -1032,9 +1076,7 @@ static int step_host_overlapped(gcs_ctx* c, const gcs_params* p, Star* host) {
     // what is left (a chunk that was never signalled is reported).
     bool missing = false;
     for (int k = 0; k < chunks && !rc; ++k) {
-        const int g0 = k < head_chunks ? k * hpc : head_groups + (k - head_chunks) * tpc;
-        const int g1 = k < head_chunks ? std::min((k + 1) * hpc, head_groups)
-                                       : std::min(head_groups + (k - head_chunks + 1) * tpc, ng);
+        const int g0 = bound[(size_t)k], g1 = bound[(size_t)k + 1];
         const int64_t first = c->h_group_start[(size_t)g0];
         const int64_t end = g1 < ng ? c->h_group_start[(size_t)g1] : c->n;
         for (uint32_t polls = 1;; ++polls) {

@@ -162,11 +162,13 @@ constexpr int kWalkMaxBatch = 64;  // nodes popped per walk round
 // are written, applies the kick/drift to the group's particles out of place
 // (pos/vel_in -> pos_out/vel_out, so the walk's other warps keep reading the
 // step's positions) and writes their Star records.  Groups are counted in
-// chunks of consecutive groups: `head_chunks` chunks of `head_per_chunk`
-// over the first `head_groups` groups, then chunks of `tail_per_chunk` over
-// the rest (the groups still in flight when the work queue runs dry, which
-// finish together at the end of the walk: small chunks there spread their
-// completions out).  The warp that completes a chunk stores `epoch` into
+// chunks of consecutive groups: chunk k is groups [chunk_bound[k],
+// chunk_bound[k + 1]) of n_chunks (the host makes large chunks over the groups
+// handed out early and small ones over the groups still in flight when the
+// work queue runs dry, which finish together at the end of the walk, and
+// puts every boundary at a super-group edge, so that a chunk's particles are
+// one contiguous range also when groups take their targets through a
+// partition of their super-group).  The warp that completes a chunk stores `epoch` into
 // host_flags[chunk] (mapped host memory, after a system-scope fence), so the
 // host can copy that chunk's Stars while the walk continues; with
 // host_flags == nullptr nothing is counted (the records go straight to
@@ -179,17 +181,16 @@ struct WalkEpilogue {
     float4* stars = nullptr;  // Star records as float4 pairs
     float dt = 0.0f;
     int32_t recolor = 0;
-    int32_t head_groups = 0;
-    int32_t head_per_chunk = 1;
-    int32_t head_chunks = 0;
-    int32_t tail_per_chunk = 1;
+    int32_t n_chunks = 0;
     uint32_t* chunk_done = nullptr;
     uint32_t* host_flags = nullptr;
     uint32_t epoch = 0;
+    int32_t chunk_bound[65] = {};  // kMaxStarChunks + 1 group indices
 };
 constexpr int kMaxStarHeadChunks = 16;
 constexpr int kMaxStarTailChunks = 48;
 constexpr int kMaxStarChunks = kMaxStarHeadChunks + kMaxStarTailChunks;
+static_assert(kMaxStarChunks + 1 == sizeof(WalkEpilogue::chunk_bound) / sizeof(int32_t), "chunk table size");
 constexpr int kWalkBlockWarps = 8;  // warps per walk block
 
 // ---- walk frontiers ------------------------------------------------------
@@ -223,6 +224,14 @@ struct WalkFrontier {
     int32_t* list = nullptr;  // [n_supers][kSuperCap]
     int32_t* src = nullptr;   // [n_supers][kSuperSrcCap] sorted particle indices
     int4* meta = nullptr;     // per super-group: n_take, n_src, n_front, valid
+    // Targets in group order (null: Morton order).  A full super-group of
+    // kSuperTargets targets is split into its groups by recursive median
+    // bisection along the longest axis of each part's box, so the groups are
+    // spatially tighter than runs of the Morton order (fewer nodes that
+    // only some of a group's targets accept); group g takes targets
+    // perm[start .. start + count).  Partial super-groups keep Morton order.
+    int32_t* perm = nullptr;
+    int32_t split_levels = 0;  // bisection levels: kSuperTargets >> levels == group width
 };
 
 void launch_walk(const Layout& L, const WalkParams& wp, const float4* pos,

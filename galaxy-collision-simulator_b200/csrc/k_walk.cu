@@ -345,7 +345,11 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
 #pragma unroll
         for (int t = 0; t < T; ++t) {
             valid[t] = lane + 32 * t < grp.count;
-            const float4 p = valid[t] ? __ldg(pos + grp.start + lane + 32 * t) : make_float4(0.f, 0.f, 0.f, 0.f);
+            float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (valid[t]) {
+                const int j = grp.start + lane + 32 * t;
+                p = __ldg(pos + (fr.perm ? __ldg(fr.perm + j) : j));
+            }
             live[t] = __ballot_sync(kFull, valid[t]);
             X.npx[t] = make_float2(-p.x, -p.x);
             X.npy[t] = make_float2(-p.y, -p.y);
@@ -705,7 +709,8 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
 #pragma unroll
         for (int t = 0; t < T; ++t) {
             if (!valid[t]) continue;
-            const int64_t i = grp.start + lane + 32 * t;
+            const int j = grp.start + lane + 32 * t;
+            const int64_t i = fr.perm ? __ldg(fr.perm + j) : j;  // the target's particle
             const float4 a = make_float4(__fadd_rn(A[t].ax.x, A[t].ax.y), __fadd_rn(A[t].ay.x, A[t].ay.y),
                                          __fadd_rn(A[t].az.x, A[t].az.y), __fadd_rn(A[t].pot.x, A[t].pot.y));
             acc[i] = a;
@@ -726,15 +731,15 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
             __syncwarp();
             if (lane == 0) {
                 __threadfence();
-                int k, in_chunk;
-                if (g < ep.head_groups) {
-                    k = g / ep.head_per_chunk;
-                    in_chunk = min(ep.head_per_chunk, ep.head_groups - k * ep.head_per_chunk);
-                } else {
-                    const int j = (g - ep.head_groups) / ep.tail_per_chunk;
-                    k = ep.head_chunks + j;
-                    in_chunk = min(ep.tail_per_chunk, n_groups - ep.head_groups - j * ep.tail_per_chunk);
+                // the chunk holding group g: the last boundary <= g
+                int lo = 0, hi = ep.n_chunks - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (ep.chunk_bound[mid] <= g) lo = mid;
+                    else hi = mid - 1;
                 }
+                const int k = lo;
+                const int in_chunk = ep.chunk_bound[k + 1] - ep.chunk_bound[k];
                 if (atomicAdd(ep.chunk_done + k, 1u) == (uint32_t)in_chunk - 1u) {
                     __threadfence_system();
                     *reinterpret_cast<volatile uint32_t*>(ep.host_flags + k) = ep.epoch;
@@ -776,6 +781,97 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
             __threadfence();
         }
     }
+}
+
+// Group partition of full super-groups (WalkFrontier::perm): one block of
+// kSuperTargets threads per super-group, one target per thread.  Each level
+// halves every part: the part's box comes from a warp reduction (and, for
+// parts wider than a warp, the part's warps through shared memory), and the
+// part is sorted by (coordinate along the box's longest axis, target) with a
+// bitonic network - shared memory for strides of 32 and more, warp shuffles
+// below - so its lower and upper halves are the two sides of the median.
+// After `levels` levels the parts are the groups.  Keys are unique, so the
+// partition is a deterministic function of the positions.
+constexpr int kPartThreads = kSuperTargets;
+static_assert(kSuperTargets == 256, "a partition thread per target; keys carry 8-bit target indices");
+
+__global__ void __launch_bounds__(kPartThreads)
+partition_kernel(const float4* __restrict__ pos, const SuperGroup* __restrict__ supers, int levels,
+                 int32_t* __restrict__ perm) {
+    __shared__ float sp[3][kPartThreads];
+    __shared__ float wlo[kPartThreads / 32][3], whi[kPartThreads / 32][3];
+    __shared__ unsigned long long skey[kPartThreads];
+    const SuperGroup sg = supers[blockIdx.x];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    if (sg.count != kSuperTargets) {  // a partial super-group keeps Morton order
+        if (t < sg.count) perm[sg.start + t] = sg.start + t;
+        return;
+    }
+    const float4 p0 = __ldg(pos + sg.start + t);
+    sp[0][t] = p0.x;
+    sp[1][t] = p0.y;
+    sp[2][t] = p0.z;
+    int e = t;  // the target this thread holds (index within the super-group)
+    __syncthreads();
+    for (int level = 0; level < levels; ++level) {
+        const int part = kPartThreads >> level;
+        const float c[3] = {sp[0][e], sp[1][e], sp[2][e]};
+        float lo[3] = {c[0], c[1], c[2]}, hi[3] = {c[0], c[1], c[2]};
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            if (o < part) {
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    lo[a] = fminf(lo[a], __shfl_xor_sync(kFull, lo[a], o));
+                    hi[a] = fmaxf(hi[a], __shfl_xor_sync(kFull, hi[a], o));
+                }
+            }
+        }
+        if (part > 32) {
+            if (lane == 0) {
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    wlo[warp][a] = lo[a];
+                    whi[warp][a] = hi[a];
+                }
+            }
+            __syncthreads();
+            const int w0 = (t / part) * (part / 32);
+            for (int w = w0; w < w0 + part / 32; ++w) {
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    lo[a] = fminf(lo[a], wlo[w][a]);
+                    hi[a] = fmaxf(hi[a], whi[w][a]);
+                }
+            }
+            __syncthreads();
+        }
+        int ax = 0;
+        float ext = hi[0] - lo[0];
+        if (hi[1] - lo[1] > ext) {
+            ax = 1;
+            ext = hi[1] - lo[1];
+        }
+        if (hi[2] - lo[2] > ext) ax = 2;
+        unsigned long long key = ((unsigned long long)float_to_ordered(c[ax]) << 8) | (unsigned long long)e;
+        for (int k = 2; k <= part; k <<= 1) {
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                unsigned long long other;
+                if (j >= 32) {
+                    skey[t] = key;
+                    __syncthreads();
+                    other = skey[t ^ j];
+                    __syncthreads();
+                } else {
+                    other = __shfl_xor_sync(kFull, key, j);
+                }
+                const bool ascending = (t & k) == 0, lower = (t & j) == 0;
+                key = (lower == ascending) ? (key < other ? key : other) : (key < other ? other : key);
+            }
+        }
+        e = (int)(key & 0xFFu);
+    }
+    perm[sg.start + t] = sg.start + e;
 }
 
 // Frontier pass (WalkFrontier, gcs_internal.h): one warp per super-group
@@ -1025,9 +1121,15 @@ void launch_walk(const Layout& L, const WalkParams& wp, const float4* pos,
     WalkFrontier fr = fr_in;
     if (fr.supers && fr.n_supers > 0 && fr.list && fr.src && fr.meta) {
         const unsigned fb = (unsigned)((fr.n_supers + kFrontWarps - 1) / kFrontWarps);
+        if (fr.perm && fr.split_levels > 0)
+            partition_kernel<<<(unsigned)fr.n_supers, kPartThreads, 0, st>>>(pos, fr.supers, fr.split_levels,
+                                                                          fr.perm);
+        else
+            fr.perm = nullptr;
         frontier_kernel<<<fb, kFrontWarps * 32, 0, st>>>(L, pos, wn, fr, wp.eps2, wp.theta2, status);
     } else {
-        fr.meta = nullptr;  // every group walks from its root
+        fr.meta = nullptr;  // every group walks from its root, targets in Morton order
+        fr.perm = nullptr;
     }
     WalkParams q = wp;
     if (q.batch < 1) q.batch = 1;

@@ -29,7 +29,7 @@ def test_two_slices_equal_one_context(gcs_mod, width, graphs):
     stars = small_collision(3000, 700, 300, seed=41)  # 8,000 particles
     n = len(stars)
     p = _params(gcs)
-    length, slices = bench.shard_slices(n, 2, 64)
+    length, slices = bench.shard_slices(n, 2, 256)
     s = torch.cuda.Stream()
     with gcs.Context(2 * length) as a, gcs.Context(2 * length) as b, gcs.Context(n) as whole:
         for ctx, (first, count) in ((a, slices[0]), (b, slices[1])):
@@ -70,9 +70,16 @@ def test_step_range_bounds_are_checked(gcs_mod):
             ctx.set_step_range(17, 64)          # not a group start
         with pytest.raises(gcs.GcsError):
             ctx.set_step_range(0, n + 32)       # past the particles
-        ctx.set_step_range(64, n - 64)          # to the end: fine
         with pytest.raises(gcs.GcsError):
-            ctx.set_group_width(48)             # 64 is not a multiple of 48
+            ctx.set_step_range(64, n - 64)      # splits a partitioned super-group of 256
+        ctx.set_walk_frontier(False)
+        ctx.set_step_range(64, n - 64)          # plain groups: a group start is enough
+        with pytest.raises(gcs.GcsError):
+            ctx.set_walk_frontier(True)         # would partition across the range's start
+        ctx.set_step_range(256, n - 256)        # to the end, on a super-group start: fine
+        ctx.set_walk_frontier(True)
+        with pytest.raises(gcs.GcsError):
+            ctx.set_group_width(48)             # 256 is not a multiple of 48
         ctx.set_group_width(16)
         ctx.set_step_range(0, -1)               # every particle again
         assert ctx.device_array(gcs.BUF_POS) != ctx.device_array(gcs.BUF_VEL)
@@ -100,7 +107,7 @@ def _slice_rank(rank, world, port, steps, out):
         import gcs
         stars = small_collision(3000, 700, 300, seed=41)  # 8,000 particles
         n = len(stars)
-        length, slices = bench.shard_slices(n, world, 64)
+        length, slices = bench.shard_slices(n, world, 256)
         first, count = slices[rank]
         with gcs.Context(world * length) as ctx:
             ctx.set_segments([n])
