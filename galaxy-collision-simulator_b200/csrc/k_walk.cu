@@ -783,68 +783,65 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
     }
 }
 
-// Group partition of full super-groups (WalkFrontier::perm): one block of
-// kSuperTargets threads per super-group, one target per thread.  Each level
-// halves every part: the part's box comes from a warp reduction (and, for
-// parts wider than a warp, the part's warps through shared memory), and the
-// part is sorted by (coordinate along the box's longest axis, target) with a
-// bitonic network - shared memory for strides of 32 and more, warp shuffles
-// below - so its lower and upper halves are the two sides of the median.
-// After `levels` levels the parts are the groups.  Keys are unique, so the
-// partition is a deterministic function of the positions.
-constexpr int kPartThreads = kSuperTargets;
-static_assert(kSuperTargets == 256, "a partition thread per target; keys carry 8-bit target indices");
+// Group partition of full super-groups (WalkFrontier::perm): one warp per
+// super-group, its kSuperTargets targets held 8 per lane (element i = lane *
+// 8 + r in register r).  Each level halves every part: the part's box comes
+// from the lane's 8 elements and a shuffle reduction over the part's lanes,
+// and the part is sorted by its coordinate along the box's longest axis with
+// a bitonic network (register pairs inside a lane, shuffles across lanes), so
+// its lower and upper halves are the two sides of the median.  After `levels`
+// levels the parts are the groups.  Keys are the coordinate's order-preserving
+// bits with the low 8 replaced by the target's index: unique, so the
+// partition is a deterministic function of the positions (targets whose
+// coordinates agree to 24 bits split by index, which only moves the median).
+constexpr int kPartWarps = 8;
+constexpr int kPartPerLane = kSuperTargets / 32;
+static_assert(kSuperTargets == 256 && kPartPerLane == 8, "8 targets per lane; keys carry 8-bit target indices");
 
-__global__ void __launch_bounds__(kPartThreads)
-partition_kernel(const float4* __restrict__ pos, const SuperGroup* __restrict__ supers, int levels,
+__global__ void __launch_bounds__(kPartWarps * 32)
+partition_kernel(const float4* __restrict__ pos, const SuperGroup* __restrict__ supers, int n_supers, int levels,
                  int32_t* __restrict__ perm) {
-    __shared__ float sp[3][kPartThreads];
-    __shared__ float wlo[kPartThreads / 32][3], whi[kPartThreads / 32][3];
-    __shared__ unsigned long long skey[kPartThreads];
-    const SuperGroup sg = supers[blockIdx.x];
-    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    __shared__ float sp[kPartWarps][3][kSuperTargets];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int sgi = blockIdx.x * kPartWarps + warp;
+    if (sgi >= n_supers) return;
+    const SuperGroup sg = supers[sgi];
     if (sg.count != kSuperTargets) {  // a partial super-group keeps Morton order
-        if (t < sg.count) perm[sg.start + t] = sg.start + t;
+        for (int i = lane; i < sg.count; i += 32) perm[sg.start + i] = sg.start + i;
         return;
     }
-    const float4 p0 = __ldg(pos + sg.start + t);
-    sp[0][t] = p0.x;
-    sp[1][t] = p0.y;
-    sp[2][t] = p0.z;
-    int e = t;  // the target this thread holds (index within the super-group)
-    __syncthreads();
+    float(*P)[kSuperTargets] = sp[warp];
+    for (int i = lane; i < kSuperTargets; i += 32) {
+        const float4 p = __ldg(pos + sg.start + i);
+        P[0][i] = p.x;
+        P[1][i] = p.y;
+        P[2][i] = p.z;
+    }
+    __syncwarp();
+    int e[kPartPerLane];
+#pragma unroll
+    for (int r = 0; r < kPartPerLane; ++r) e[r] = lane * kPartPerLane + r;
     for (int level = 0; level < levels; ++level) {
-        const int part = kPartThreads >> level;
-        const float c[3] = {sp[0][e], sp[1][e], sp[2][e]};
-        float lo[3] = {c[0], c[1], c[2]}, hi[3] = {c[0], c[1], c[2]};
+        const int part = kSuperTargets >> level;
+        const int part_lanes = part / kPartPerLane;
+        float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+#pragma unroll
+        for (int r = 0; r < kPartPerLane; ++r)
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                const float v = P[a][e[r]];
+                lo[a] = fminf(lo[a], v);
+                hi[a] = fmaxf(hi[a], v);
+            }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
-            if (o < part) {
+            if (o < part_lanes) {
 #pragma unroll
                 for (int a = 0; a < 3; ++a) {
                     lo[a] = fminf(lo[a], __shfl_xor_sync(kFull, lo[a], o));
                     hi[a] = fmaxf(hi[a], __shfl_xor_sync(kFull, hi[a], o));
                 }
             }
-        }
-        if (part > 32) {
-            if (lane == 0) {
-#pragma unroll
-                for (int a = 0; a < 3; ++a) {
-                    wlo[warp][a] = lo[a];
-                    whi[warp][a] = hi[a];
-                }
-            }
-            __syncthreads();
-            const int w0 = (t / part) * (part / 32);
-            for (int w = w0; w < w0 + part / 32; ++w) {
-#pragma unroll
-                for (int a = 0; a < 3; ++a) {
-                    lo[a] = fminf(lo[a], wlo[w][a]);
-                    hi[a] = fmaxf(hi[a], whi[w][a]);
-                }
-            }
-            __syncthreads();
         }
         int ax = 0;
         float ext = hi[0] - lo[0];
@@ -853,25 +850,41 @@ partition_kernel(const float4* __restrict__ pos, const SuperGroup* __restrict__ 
             ext = hi[1] - lo[1];
         }
         if (hi[2] - lo[2] > ext) ax = 2;
-        unsigned long long key = ((unsigned long long)float_to_ordered(c[ax]) << 8) | (unsigned long long)e;
-        for (int k = 2; k <= part; k <<= 1) {
+        uint32_t key[kPartPerLane];
+#pragma unroll
+        for (int r = 0; r < kPartPerLane; ++r)
+            key[r] = (float_to_ordered(P[ax][e[r]]) & 0xFFFFFF00u) | (uint32_t)e[r];
+#pragma unroll
+        for (int k = 2; k <= kSuperTargets; k <<= 1) {
+            if (k > part) continue;  // uniform; the loops stay unrolled, register indices constant
+#pragma unroll
             for (int j = k >> 1; j > 0; j >>= 1) {
-                unsigned long long other;
-                if (j >= 32) {
-                    skey[t] = key;
-                    __syncthreads();
-                    other = skey[t ^ j];
-                    __syncthreads();
-                } else {
-                    other = __shfl_xor_sync(kFull, key, j);
+                if (j >= kPartPerLane) {  // partner in lane ^ (j / 8), same register
+                    const int lj = j / kPartPerLane;
+                    const bool lower = (lane & lj) == 0;
+#pragma unroll
+                    for (int r = 0; r < kPartPerLane; ++r) {
+                        const uint32_t other = __shfl_xor_sync(kFull, key[r], lj);
+                        const bool ascending = ((lane * kPartPerLane + r) & k) == 0;
+                        key[r] = (lower == ascending) ? min(key[r], other) : max(key[r], other);
+                    }
+                } else {  // partner in register r ^ j of this lane
+#pragma unroll
+                    for (int r = 0; r < kPartPerLane; ++r) {
+                        if ((r & j) != 0) continue;
+                        const bool ascending = ((lane * kPartPerLane + r) & k) == 0;
+                        const uint32_t a = key[r], b = key[r | j];
+                        key[r] = ascending ? min(a, b) : max(a, b);
+                        key[r | j] = ascending ? max(a, b) : min(a, b);
+                    }
                 }
-                const bool ascending = (t & k) == 0, lower = (t & j) == 0;
-                key = (lower == ascending) ? (key < other ? key : other) : (key < other ? other : key);
             }
         }
-        e = (int)(key & 0xFFu);
+#pragma unroll
+        for (int r = 0; r < kPartPerLane; ++r) e[r] = (int)(key[r] & 0xFFu);
     }
-    perm[sg.start + t] = sg.start + e;
+#pragma unroll
+    for (int r = 0; r < kPartPerLane; ++r) perm[sg.start + lane * kPartPerLane + r] = sg.start + e[r];
 }
 
 // Frontier pass (WalkFrontier, gcs_internal.h): one warp per super-group
@@ -1122,8 +1135,8 @@ void launch_walk(const Layout& L, const WalkParams& wp, const float4* pos,
     if (fr.supers && fr.n_supers > 0 && fr.list && fr.src && fr.meta) {
         const unsigned fb = (unsigned)((fr.n_supers + kFrontWarps - 1) / kFrontWarps);
         if (fr.perm && fr.split_levels > 0)
-            partition_kernel<<<(unsigned)fr.n_supers, kPartThreads, 0, st>>>(pos, fr.supers, fr.split_levels,
-                                                                          fr.perm);
+            partition_kernel<<<(unsigned)((fr.n_supers + kPartWarps - 1) / kPartWarps), kPartWarps * 32, 0, st>>>(
+                pos, fr.supers, fr.n_supers, fr.split_levels, fr.perm);
         else
             fr.perm = nullptr;
         frontier_kernel<<<fb, kFrontWarps * 32, 0, st>>>(L, pos, wn, fr, wp.eps2, wp.theta2, status);
