@@ -71,6 +71,10 @@ struct gcs_ctx {
     int n_supers = 0;
     size_t supers_cap = 0;
     int32_t* perm = nullptr;              // walk targets in group order (full super-groups partitioned)
+    // second stream and events for the partition beside the frontier pass
+    // (created at the first partitioned walk and kept)
+    cudaStream_t part_stream = nullptr;
+    cudaEvent_t part_fork = nullptr, part_join = nullptr;
     std::vector<int32_t> h_group_super;   // super-group of each walk group (host copy)
     Chunk* chunks = nullptr;
     float2* seg_bounds = nullptr;
@@ -230,6 +234,12 @@ void free_all(gcs_ctx* c) {
         cudaStreamDestroy(c->star_stream);
     }
     if (c->star_walked) cudaEventDestroy(c->star_walked);
+    if (c->part_stream) {
+        cudaStreamSynchronize(c->part_stream);
+        cudaStreamDestroy(c->part_stream);
+    }
+    if (c->part_fork) cudaEventDestroy(c->part_fork);
+    if (c->part_join) cudaEventDestroy(c->part_join);
     if (c->star_flags) cudaFreeHost(c->star_flags);
     void* ptrs[] = {c->pos[0], c->pos[1], c->vel[0], c->vel[1], c->acc, c->keys[0], c->keys[1],
                     c->idx[0], c->idx[1], c->tr, c->bd, c->wn, c->com64, c->leaf_parent, c->seg_off,
@@ -364,6 +374,20 @@ int upload_groups(gcs_ctx* c) {
 
 }  // namespace
 
+// The partition's second stream and its fork/join events, created once per
+// context (before any capture of the step: build_step_graphs calls it too).
+static int ensure_part_stream(gcs_ctx* c) {
+    if (c->part_stream) return GCS_OK;
+    cudaSetDevice(c->device);
+    if (cudaStreamCreateWithFlags(&c->part_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->part_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->part_join, cudaEventDisableTiming) != cudaSuccess) {
+        set_error(c, "partition stream", cudaGetLastError());
+        return GCS_ERR_CUDA;
+    }
+    return GCS_OK;
+}
+
 // ---------------------------------------------------------------------------
 // stage sequence
 // ---------------------------------------------------------------------------
@@ -395,6 +419,13 @@ static int walk_stage(gcs_ctx* c, const gcs_params* p, const WalkEpilogue& ep) {
     fr.meta = c->sg_meta;
     fr.perm = partitioned(c) ? c->perm : nullptr;
     fr.split_levels = split_levels(c->group_width);
+    if (fr.perm) {
+        const int rc = ensure_part_stream(c);
+        if (rc) return rc;
+        fr.side = c->part_stream;
+        fr.fork = c->part_fork;
+        fr.join = c->part_join;
+    }
     launch_walk(L, wp, c->pos[c->cur], c->wn, c->groups, c->n_groups, c->group_width > 32 ? 2 : 1, c->acc,
                 scratch_at<uint32_t>(c, sl.walk_q), c->status, p->walk_blocks_per_sm, c->sm_count,
                 c->count_walk ? c->counts : nullptr, c->walk_stack, c->walk_stack_entries, st, ep, fr);
@@ -868,7 +899,8 @@ int gcs_download_playback(gcs_ctx* c, PlaybackStar* host, int64_t offset, int64_
 static int build_step_graphs(gcs_ctx* c, const gcs_params* p) {
     drop_graphs(c);
     const int cur0 = c->cur;
-    int rc = GCS_OK;
+    int rc = partitioned(c) ? ensure_part_stream(c) : GCS_OK;
+    if (rc) return rc;
     for (int k = 0; k < 2 && !rc; ++k) {
         const int parity = cur0 ^ k;
         c->cur = parity;

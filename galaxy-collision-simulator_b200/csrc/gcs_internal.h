@@ -232,6 +232,11 @@ struct WalkFrontier {
     // perm[start .. start + count).  Partial super-groups keep Morton order.
     int32_t* perm = nullptr;
     int32_t split_levels = 0;  // bisection levels: kSuperTargets >> levels == group width
+    // Optional second stream for the partition: forked from the walk's stream
+    // with `fork`, joined back with `join` before the walk, so it runs beside
+    // the frontier pass (both are short latency chains).
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
 };
 
 void launch_walk(const Layout& L, const WalkParams& wp, const float4* pos,

@@ -1134,12 +1134,24 @@ void launch_walk(const Layout& L, const WalkParams& wp, const float4* pos,
     WalkFrontier fr = fr_in;
     if (fr.supers && fr.n_supers > 0 && fr.list && fr.src && fr.meta) {
         const unsigned fb = (unsigned)((fr.n_supers + kFrontWarps - 1) / kFrontWarps);
-        if (fr.perm && fr.split_levels > 0)
-            partition_kernel<<<(unsigned)((fr.n_supers + kPartWarps - 1) / kPartWarps), kPartWarps * 32, 0, st>>>(
-                pos, fr.supers, fr.n_supers, fr.split_levels, fr.perm);
-        else
+        bool joined = false;
+        if (fr.perm && fr.split_levels > 0) {
+            const unsigned pb = (unsigned)((fr.n_supers + kPartWarps - 1) / kPartWarps);
+            if (fr.side && fr.fork && fr.join && cudaEventRecord(fr.fork, st) == cudaSuccess &&
+                cudaStreamWaitEvent(fr.side, fr.fork, 0) == cudaSuccess) {
+                partition_kernel<<<pb, kPartWarps * 32, 0, fr.side>>>(pos, fr.supers, fr.n_supers, fr.split_levels,
+                                                                      fr.perm);
+                cudaEventRecord(fr.join, fr.side);
+                joined = true;
+            } else {
+                partition_kernel<<<pb, kPartWarps * 32, 0, st>>>(pos, fr.supers, fr.n_supers, fr.split_levels,
+                                                                 fr.perm);
+            }
+        } else {
             fr.perm = nullptr;
+        }
         frontier_kernel<<<fb, kFrontWarps * 32, 0, st>>>(L, pos, wn, fr, wp.eps2, wp.theta2, status);
+        if (joined) cudaStreamWaitEvent(st, fr.join, 0);
     } else {
         fr.meta = nullptr;  // every group walks from its root, targets in Morton order
         fr.perm = nullptr;
