@@ -960,20 +960,18 @@ def main():
     ctx.download(out=hv)
     ke = max(1, args.e2e_steps)
     for _ in range(max(1, args.warmup)):  # untimed: the host step's copy stream and flags are made here
-        ctx.upload(hv)
-        ctx.step_host(p, hv)
+        ctx.step_host_io(p, hv, hv)
     torch.cuda.synchronize()
     barrier()
     t0 = time.perf_counter()
     for _ in range(ke):
-        ctx.upload(hv)
-        ctx.step_host(p, hv)
+        ctx.step_host_io(p, hv, hv)
     t_e2e = time.perf_counter() - t0
     e2e_value, t_e2e, _ = replica_throughput(n, ke, t_e2e, dist, "cuda")
     e2e = {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": 32 * n,
            "d2h_bytes_per_step": 32 * n, "steps": ke,
-           "path": "gcs_upload_stars (pinned Star[] H2D) + gcs_step_host (step; Star[] D2H of each finished "
-                   "chunk of walk groups, overlapped with the walk)"}
+           "path": "gcs_step_host_io: pinned Star[] H2D in chunks, each unpacked and reduced into the bounds as "
+                   "it lands; step; Star[] D2H written by the walk's warps while the walk runs"}
 
     peaks = measured_peaks()
     sm_max = float(peaks.get("sm_max_mhz", 1965.0))

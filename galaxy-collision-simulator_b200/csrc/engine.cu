@@ -36,6 +36,7 @@ struct gcs_ctx {
     int32_t n = 0, nseg = 0, n_internal = 0;
     std::vector<int64_t> h_seg_off;
     std::vector<int32_t> h_group_start;  // first particle of each walk group (host copy)
+    std::vector<int64_t> h_chunk_first;  // first particle of each bounds chunk, then n (host copy)
     int n_groups = 0, n_chunks = 0;
 
     // device state
@@ -106,6 +107,7 @@ struct gcs_ctx {
     // mapped host memory (written by the walk's epilogue) and their device
     // counters; created at the first such step and kept
     cudaStream_t star_stream = nullptr;
+    cudaEvent_t up_landed[8] = {};       // chunks of the step's Star upload (gcs_step_host_io)
     cudaEvent_t star_walked = nullptr;
     uint32_t* star_flags = nullptr;      // mapped host memory, kMaxStarChunks words
     uint32_t* star_flags_dev = nullptr;  // its device address
@@ -234,6 +236,8 @@ void free_all(gcs_ctx* c) {
         cudaStreamDestroy(c->star_stream);
     }
     if (c->star_walked) cudaEventDestroy(c->star_walked);
+    for (cudaEvent_t e : c->up_landed)
+        if (e) cudaEventDestroy(e);
     if (c->part_stream) {
         cudaStreamSynchronize(c->part_stream);
         cudaStreamDestroy(c->part_stream);
@@ -747,6 +751,9 @@ static int apply_layout(gcs_ctx* c, int32_t num_segments, const int64_t* counts)
     GCS_CUDA(c, cudaMemcpyAsync(c->chunks, chunks.data(), sizeof(Chunk) * chunks.size(),
                                 cudaMemcpyHostToDevice, c->stream));
     c->h_seg_off = off;
+    c->h_chunk_first.clear();
+    for (const Chunk& ch : chunks) c->h_chunk_first.push_back(ch.start);
+    c->h_chunk_first.push_back(n);
     c->n = (int32_t)n;
     c->nseg = num_segments;
     c->n_internal = (int32_t)(n - num_segments);
@@ -1011,6 +1018,8 @@ static void* mapped_host_range(const void* p, size_t bytes) {
 static int ensure_star_pipeline(gcs_ctx* c) {
     if (!c->star_stream) GCS_CUDA(c, cudaStreamCreateWithFlags(&c->star_stream, cudaStreamNonBlocking));
     if (!c->star_walked) GCS_CUDA(c, cudaEventCreateWithFlags(&c->star_walked, cudaEventDisableTiming));
+    for (cudaEvent_t& e : c->up_landed)
+        if (!e) GCS_CUDA(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     if (!c->star_flags) {
         GCS_CUDA(c, cudaHostAlloc(reinterpret_cast<void**>(&c->star_flags), sizeof(uint32_t) * kMaxStarChunks,
                                   cudaHostAllocMapped));
@@ -1035,8 +1044,8 @@ static int ensure_star_pipeline(gcs_ctx* c) {
 // completions, and copies, spread over the walk's last phase.  The result is the
 // same bits as the plain stage sequence followed by gcs_download_stars.  A
 // step range (one slice of the scenario) takes that plain sequence.
-static int step_host_overlapped(gcs_ctx* c, const gcs_params* p, Star* host) {
-    int rc = run_stages(c, p, GCS_STAGE_BOUNDS, GCS_STAGE_AGGREGATE);
+static int step_host_overlapped(gcs_ctx* c, const gcs_params* p, Star* host, int first_stage = GCS_STAGE_BOUNDS) {
+    int rc = run_stages(c, p, first_stage, GCS_STAGE_AGGREGATE);
     if (rc) return rc;
     // A pinned, device-mapped host array: the epilogue writes each group's
     // Stars straight into it over PCIe while the walk goes on (no copies, no
@@ -1147,6 +1156,54 @@ static int step_host_overlapped(gcs_ctx* c, const gcs_params* p, Star* host) {
         return GCS_ERR_STATE;
     }
     return GCS_OK;
+}
+
+// One step from host Stars to host Stars.  The upload goes in up to 8 chunks
+// (whole bounds chunks) on the copy stream; the context stream unpacks each
+// chunk, and reduces it into the segment bounds when the bounds come from
+// the device, as soon as it has landed, so the PCIe copy overlaps that work
+// and no host synchronisation separates the upload from the step; the rest
+// is gcs_step_host's step (Stars back while the walk runs).
+int gcs_step_host_io(gcs_ctx* c, const gcs_params* p, const Star* in, Star* out) {
+    if (!c || !in || !out) return GCS_ERR_ARG;
+    cudaSetDevice(c->device);
+    int rc = validate_params(c, p);
+    if (rc) return rc;
+    if (c->range_count >= 0 || c->n_groups <= 0 || c->n <= 0 || c->n_chunks <= 0) {
+        rc = gcs_upload_stars(c, in, 0, c->n);
+        return rc ? rc : gcs_step_host(c, p, out);
+    }
+    rc = ensure_star_pipeline(c);
+    if (rc) return rc;
+    const bool device_bounds = p->bounds_mode == GCS_BOUNDS_DEVICE;
+    const Layout L = layout_of(c);
+    const ScratchLayout sl = scratch_layout(c->max_segments, c->n, c->nseg);
+    uint32_t* enc = scratch_at<uint32_t>(c, sl.bounds);
+    if (device_bounds) GCS_CUDA(c, cudaMemsetAsync(enc, 0, sizeof(uint32_t) * 2 * (size_t)c->nseg, c->stream));
+    // the copy stream starts after everything queued so far (the previous
+    // step may still be reading the staging buffer and the particle arrays)
+    GCS_CUDA(c, cudaEventRecord(c->up_landed[0], c->stream));
+    GCS_CUDA(c, cudaStreamWaitEvent(c->star_stream, c->up_landed[0], 0));
+    constexpr int kUpChunks = (int)(sizeof(c->up_landed) / sizeof(c->up_landed[0]));
+    const int per = (c->n_chunks + kUpChunks - 1) / kUpChunks;
+    for (int u = 0, e0 = 0; e0 < c->n_chunks; ++u, e0 += per) {
+        const int e1 = std::min(e0 + per, c->n_chunks);
+        const int64_t a = c->h_chunk_first[(size_t)e0], b = c->h_chunk_first[(size_t)e1];
+        GCS_CUDA(c, cudaMemcpyAsync(c->staging + a, in + a, sizeof(Star) * (size_t)(b - a), cudaMemcpyHostToDevice,
+                                    c->star_stream));
+        GCS_CUDA(c, cudaEventRecord(c->up_landed[u], c->star_stream));
+        GCS_CUDA(c, cudaStreamWaitEvent(c->stream, c->up_landed[u], 0));
+        launch_unpack_stars(c->staging + a, c->pos[c->cur] + a, c->vel[c->cur] + a, b - a, c->stream);
+        if (device_bounds) launch_bounds(L, c->pos[c->cur], c->chunks + e0, e1 - e0, enc, c->status, c->stream);
+        rc = check_launch(c, "upload chunk");
+        if (rc) return rc;
+    }
+    if (device_bounds) {
+        launch_bounds_decode(enc, c->seg_bounds, c->nseg, c->stream);
+        rc = check_launch(c, "bounds");
+        if (rc) return rc;
+    }
+    return step_host_overlapped(c, p, out, GCS_STAGE_ENCODE);
 }
 
 int gcs_step_host(gcs_ctx* c, const gcs_params* p, Star* host) {

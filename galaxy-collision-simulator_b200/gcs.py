@@ -106,6 +106,7 @@ def lib() -> C.CDLL:
         "gcs_download_playback": (C.c_int, [P, P, i64, i64]),
         "gcs_step": (C.c_int, [P, C.POINTER(Params)]),
         "gcs_step_host": (C.c_int, [P, C.POINTER(Params), P]),
+        "gcs_step_host_io": (C.c_int, [P, C.POINTER(Params), P, P]),
         "gcs_compute_accels": (C.c_int, [P, C.POINTER(Params)]),
         "gcs_kick": (C.c_int, [P, f32]),
         "gcs_run_stages": (C.c_int, [P, C.POINTER(Params), i32, i32]),
@@ -312,6 +313,14 @@ class Context:
         if out.dtype != STAR_DTYPE or len(out) < self.n or not out.flags.c_contiguous:
             raise ValueError("step_host needs a contiguous Star array of at least n records")
         self.check(self.L.gcs_step_host(self._h, C.byref(p), _ptr(out)))
+
+    def step_host_io(self, p: Params, inp: np.ndarray, out: np.ndarray) -> None:
+        """upload(inp) + step_host(p, out) with the upload chunked and
+        overlapped with unpacking and the bounds (`out` may be `inp`)."""
+        for a in (inp, out):
+            if a.dtype != STAR_DTYPE or len(a) < self.n or not a.flags.c_contiguous:
+                raise ValueError("step_host_io needs contiguous Star arrays of at least n records")
+        self.check(self.L.gcs_step_host_io(self._h, C.byref(p), _ptr(inp), _ptr(out)))
 
     def compute_accels(self, p: Params) -> None:
         self.check(self.L.gcs_compute_accels(self._h, C.byref(p)))

@@ -182,6 +182,14 @@ int32_t gcs_graph_builds(const gcs_ctx* ctx);
  * Stars and the device state are the same bits as
  * gcs_run_stages(bounds..integrate) followed by gcs_download_stars. */
 int gcs_step_host(gcs_ctx* ctx, const gcs_params* p, Star* host);
+/* One step from host Stars to host Stars: the same result as
+ * gcs_upload_stars(ctx, in, 0, n) followed by gcs_step_host(ctx, p, out)
+ * (`out` may be `in`), with the upload in up to 8 chunks on a copy stream,
+ * each chunk unpacked and reduced into the device bounds as soon as it lands,
+ * and no host synchronisation between the upload and the step (the
+ * reference uploads its Stars once, cuda_engine.cu:283-296, and copies them
+ * back after every step, cuda_engine.cu:442-448). */
+int gcs_step_host_io(gcs_ctx* ctx, const gcs_params* p, const Star* in, Star* out);
 /* Accelerations at the current positions (bounds..walk, no kick/drift).
  * Afterwards the particle arrays are in this step's Morton order and the
  * acceleration buffer matches them. */

@@ -185,3 +185,45 @@ def test_dropin_host_step_equals_engine_steps(gcs_mod):
                 assert host.tobytes() == b.download().tobytes()
     finally:
         cleanup()
+
+
+@pytest.mark.parametrize("pinned,same_buffer,bounds", [(True, True, "device"), (False, True, "device"),
+                                                        (True, False, "caller"), (False, False, "device")])
+def test_host_step_io_equals_upload_then_host_step(gcs_mod, pinned, same_buffer, bounds):
+    """gcs_step_host_io (chunked upload, each chunk unpacked and reduced into
+    the bounds as it lands, then the host step) gives the same Stars and the
+    same device state as gcs_upload_stars + gcs_step_host, step after step,
+    over uneven segments (chunks of the upload cross segment ends)."""
+    gcs = gcs_mod
+    parts = [small_collision(9000, 2000, 1000, seed=61), small_collision(700, 150, 60, seed=62)[:1777],
+             small_collision(20, 5, 3, seed=63)[:33]]
+    stars = np.concatenate(parts)
+    counts = [len(x) for x in parts]
+    n = len(stars)
+    p = _params(gcs)
+    if bounds == "caller":
+        pos, _ = gcs.pos_vel_from_stars(stars)
+        p.bounds_mode = gcs.BOUNDS_CALLER
+        p.global_min, p.global_max = float(pos[:, :3].min()) - 1.0, float(pos[:, :3].max()) + 1.0
+        counts = [n]
+    with gcs.Context(n, max_segments=len(counts)) as a, gcs.Context(n, max_segments=len(counts)) as b:
+        for ctx in (a, b):
+            ctx.set_segments(counts)
+        if pinned:
+            keep_in, cur = _pinned_stars(gcs, n)
+            keep_out, out = _pinned_stars(gcs, n, 16)
+        else:
+            cur, out = np.zeros(n, dtype=gcs.STAR_DTYPE), np.zeros(n, dtype=gcs.STAR_DTYPE)
+        cur[:] = stars
+        ref = stars.copy()
+        ref_out = np.zeros(n, dtype=gcs.STAR_DTYPE)
+        for _ in range(3):
+            dst = cur if same_buffer else out
+            a.step_host_io(p, cur, dst)
+            b.upload(ref)
+            b.step_host(p, ref_out)
+            assert dst.tobytes() == ref_out.tobytes()
+            assert a.download().tobytes() == b.download().tobytes()
+            cur[:] = dst
+            ref[:] = ref_out
+        assert a.device_status() == 0 and b.device_status() == 0
