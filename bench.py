@@ -922,6 +922,7 @@ def main():
                  "group_width": ctx.group_width, "walk_ms": tune_ms}
     ctx.upload(stars)
     n_mono, n_part = ctx.count_interactions(p)
+    stack_peak, stack_global = ctx.walk_stack_peak()
     ctx.upload(stars)
 
     for _ in range(args.warmup):
@@ -985,7 +986,8 @@ def main():
                 "peak_source": "derived: %d SMs x 128 FP32 lanes x 2 x sm_max_mhz %.0f (MEASURED_PEAKS.json); "
                                "no FP32 figure is measured there" % (props.multi_processor_count, sm_max),
                 "walk_ms": walk_ms, "interactions_per_step": inter, "monopole_terms": n_mono,
-                "particle_terms": n_part, "interactions_per_s": inter / (walk_ms / 1e3)}
+                "particle_terms": n_part, "interactions_per_s": inter / (walk_ms / 1e3),
+                "walk_stack_peak": stack_peak, "walk_stack_global_per_warp": stack_global}
     passes = 8
     launches_per_step = 2 + 1 + passes + 1 + 1 + 1 + 1 + 1
     line = {"metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,

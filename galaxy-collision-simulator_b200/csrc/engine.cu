@@ -139,7 +139,7 @@ struct gcs_ctx {
 namespace {
 
 constexpr int kChunkSize = 2048;  // particles per bounds block
-constexpr int kCountWords = 8;  // counting-walk outputs (gcs_count_interactions)
+constexpr int kCountWords = 9;  // counting-walk outputs: 8 for gcs_count_interactions, the stack peak
 constexpr int kMinGroupWidth = 8;
 
 size_t round256(size_t b) { return (b + 255) & ~(size_t)255; }
@@ -1335,9 +1335,20 @@ int gcs_count_interactions(gcs_ctx* c, const gcs_params* p, uint64_t out[8]) {
     const int rc = run_stages(c, p, GCS_STAGE_BOUNDS, GCS_STAGE_WALK);
     c->count_walk = false;
     if (rc) return rc;
-    GCS_CUDA(c, cudaMemcpyAsync(out, c->counts, kCountWords * sizeof(uint64_t), cudaMemcpyDeviceToHost,
+    GCS_CUDA(c, cudaMemcpyAsync(out, c->counts, 8 * sizeof(uint64_t), cudaMemcpyDeviceToHost,
                                 c->stream));
     GCS_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GCS_OK;
+}
+
+int gcs_walk_stack_peak(gcs_ctx* c, int64_t out[2]) {
+    if (!c || !out) return GCS_ERR_ARG;
+    cudaSetDevice(c->device);
+    uint64_t peak = 0;
+    GCS_CUDA(c, cudaMemcpyAsync(&peak, c->counts + 8, sizeof peak, cudaMemcpyDeviceToHost, c->stream));
+    GCS_CUDA(c, cudaStreamSynchronize(c->stream));
+    out[0] = (int64_t)peak;
+    out[1] = kWalkGlobalStack;
     return GCS_OK;
 }
 

@@ -196,6 +196,7 @@ struct WarpCount {
     uint32_t w_node, w_src;       // warp-wide node / source evaluations
     uint32_t rounds, spills;      // pop rounds, stack spills to global memory
     uint32_t all_open, all_take;  // nodes classified open / take by the box test
+    uint32_t peak;                // deepest stack (shared top + global bottom), entries
 };
 
 // Two evaluation entries for one target, packed (sm_100 f32x2): d = c - x
@@ -374,7 +375,7 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
         const int off = (int)__ldg(L.seg_off + s);
         const int seg_n = (int)__ldg(L.seg_off + s + 1) - off;
         WarpCount WC;
-        WC.w_node = WC.w_src = WC.rounds = WC.spills = WC.all_open = WC.all_take = 0u;
+        WC.w_node = WC.w_src = WC.rounds = WC.spills = WC.all_open = WC.all_take = WC.peak = 0u;
         int nsrc = 0;
 
         if (seg_n >= 2) {
@@ -543,6 +544,7 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                 }
                 __syncwarp();
                 if (kCount) {
+                    WC.peak = max(WC.peak, (uint32_t)(top + b + gtop));
                     WC.w_node += (uint32_t)b;
                     WC.rounds += 1u;
                     WC.all_open += (uint32_t)(b - n_full - n_take - n_mixed);
@@ -766,6 +768,7 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                 atomicAdd(counts + 5, (unsigned long long)WC.spills);
                 atomicAdd(counts + 6, (unsigned long long)WC.all_open);
                 atomicAdd(counts + 7, (unsigned long long)WC.all_take);
+                atomicMax(counts + 8, (unsigned long long)WC.peak);
             }
         }
         __syncwarp();

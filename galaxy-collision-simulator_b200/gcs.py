@@ -122,6 +122,7 @@ def lib() -> C.CDLL:
         "gcs_direct_accels_fp64": (C.c_int, [P, C.POINTER(Params), i32, C.POINTER(i64), i64,
                                              C.POINTER(C.c_double)]),
         "gcs_count_interactions": (C.c_int, [P, C.POINTER(Params), C.POINTER(C.c_uint64)]),
+        "gcs_walk_stack_peak": (C.c_int, [P, C.POINTER(C.c_int64)]),
         "gcs_autotune": (C.c_int, [P, C.POINTER(Params), C.POINTER(C.c_double)]),
         "gcs_set_group_width": (C.c_int, [P, i32]),
         "gcs_set_walk_frontier": (C.c_int, [P, i32]),
@@ -395,6 +396,13 @@ class Context:
         self.check(self.L.gcs_count_interactions(self._h, C.byref(p), out))
         r = tuple(int(x) for x in out)
         return r if warp_evals else r[:2]
+
+    def walk_stack_peak(self):
+        """(deepest walk stack of the last count_interactions in entries,
+        global-memory stack entries each walk warp may use)."""
+        out = (C.c_int64 * 2)()
+        self.check(self.L.gcs_walk_stack_peak(self._h, out))
+        return int(out[0]), int(out[1])
 
     def set_step_range(self, first: int, count: int) -> None:
         """Walk and kick/drift only the sorted particles [first, first + count)

@@ -300,6 +300,13 @@ int gcs_diagnostics_kicked(gcs_ctx* ctx, int32_t segment, double kick, double ou
  * global memory}, then {node evaluations opened by every active lane, node
  * evaluations accepted by every active lane}. */
 int gcs_count_interactions(gcs_ctx* ctx, const gcs_params* p, uint64_t out[8]);
+/* Deepest walk stack of the last gcs_count_interactions, in entries (one
+ * node and its target masks each), over every warp: out[0]; out[1] the
+ * entries of the global-memory bottom each walk warp may spill to (32-target
+ * groups; the shared-memory top holds a few hundred more).  Synchronises the
+ * context stream.  No counterpart in the reference, whose walk keeps a fixed
+ * 256-entry local stack per thread (cuda_engine.cu:106). */
+int gcs_walk_stack_peak(gcs_ctx* ctx, int64_t out[2]);
 /* Autotuner: times the walk on the current state for leaf sizes
  * {1,2,4,8,16,32} from p->tune_leaf_min up to p->leaf_size (the caller's
  * "leaf <= L"; leaf size 2 gives exactly the reference's terms, sizes >= 3

@@ -218,6 +218,9 @@ def test_walk_frontier_keeps_every_targets_terms(gcs_mod, oracle_mod, width, the
             _assert_acc(acc[:, :3], ref[:, :3], "frontier=%s width=%d theta=%s L=%d" % (frontier, width, theta, leaf))
             np.testing.assert_allclose(acc[:, 3], ref[:, 3], rtol=1e-5)
             assert ctx.count_interactions(p) == want, frontier
+            peak, global_cap = ctx.walk_stack_peak()
+            # the deepest stack a walk warp held fits the shared top plus the global bottom
+            assert 0 < peak <= global_cap + 512, (frontier, peak)
         assert ctx.device_status() == 0
 
 
