@@ -921,8 +921,15 @@ def main():
         tuned = {"leaf_size": p.leaf_size, "walk_batch": p.walk_batch, "blocks_per_sm": p.walk_blocks_per_sm,
                  "group_width": ctx.group_width, "walk_ms": tune_ms}
     ctx.upload(stars)
-    n_mono, n_part = ctx.count_interactions(p)
+    counted = ctx.count_interactions(p, warp_evals=True)
+    n_mono, n_part = counted[:2]
     stack_peak, stack_global = ctx.walk_stack_peak()
+    lane_use = ctx.walk_lane_use()
+    rows = (lane_use["rows_take_list"] + lane_use["rows_take_full"] + lane_use["rows_take_partial"]
+            + lane_use["rows_mixed"] + counted[3])
+    lane_use["rows_source"] = counted[3]
+    slots = 64 if ctx.group_width > 32 else 32  # target slots of a walk warp
+    lane_use["useful_lane_fraction"] = (n_mono + n_part) / (float(slots) * rows) if rows else None
     ctx.upload(stars)
 
     for _ in range(args.warmup):
@@ -987,7 +994,8 @@ def main():
                                "no FP32 figure is measured there" % (props.multi_processor_count, sm_max),
                 "walk_ms": walk_ms, "interactions_per_step": inter, "monopole_terms": n_mono,
                 "particle_terms": n_part, "interactions_per_s": inter / (walk_ms / 1e3),
-                "walk_stack_peak": stack_peak, "walk_stack_global_per_warp": stack_global}
+                "walk_stack_peak": stack_peak, "walk_stack_global_per_warp": stack_global,
+                "walk_lane_use": lane_use}
     passes = 8
     launches_per_step = 2 + 1 + passes + 1 + 1 + 1 + 1 + 1
     line = {"metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,

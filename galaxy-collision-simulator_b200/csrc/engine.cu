@@ -76,6 +76,10 @@ struct gcs_ctx {
     // (created at the first partitioned walk and kept)
     cudaStream_t part_stream = nullptr;
     cudaEvent_t part_fork = nullptr, part_join = nullptr;
+    // the gather runs on part_stream beside the tree build (both need only
+    // the sort); the build stage joins it
+    cudaEvent_t gather_fork = nullptr, gather_join = nullptr;
+    bool gather_pending = false;
     std::vector<int32_t> h_group_super;   // super-group of each walk group (host copy)
     Chunk* chunks = nullptr;
     float2* seg_bounds = nullptr;
@@ -139,7 +143,7 @@ struct gcs_ctx {
 namespace {
 
 constexpr int kChunkSize = 2048;  // particles per bounds block
-constexpr int kCountWords = 9;  // counting-walk outputs: 8 for gcs_count_interactions, the stack peak
+constexpr int kCountWords = 17;  // counting-walk outputs: gcs_count_interactions, stack peak, lane use
 constexpr int kMinGroupWidth = 8;
 
 size_t round256(size_t b) { return (b + 255) & ~(size_t)255; }
@@ -244,6 +248,8 @@ void free_all(gcs_ctx* c) {
     }
     if (c->part_fork) cudaEventDestroy(c->part_fork);
     if (c->part_join) cudaEventDestroy(c->part_join);
+    if (c->gather_fork) cudaEventDestroy(c->gather_fork);
+    if (c->gather_join) cudaEventDestroy(c->gather_join);
     if (c->star_flags) cudaFreeHost(c->star_flags);
     void* ptrs[] = {c->pos[0], c->pos[1], c->vel[0], c->vel[1], c->acc, c->keys[0], c->keys[1],
                     c->idx[0], c->idx[1], c->tr, c->bd, c->wn, c->com64, c->leaf_parent, c->seg_off,
@@ -385,7 +391,9 @@ static int ensure_part_stream(gcs_ctx* c) {
     cudaSetDevice(c->device);
     if (cudaStreamCreateWithFlags(&c->part_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->part_fork, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&c->part_join, cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventCreateWithFlags(&c->part_join, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->gather_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->gather_join, cudaEventDisableTiming) != cudaSuccess) {
         set_error(c, "partition stream", cudaGetLastError());
         return GCS_ERR_CUDA;
     }
@@ -436,7 +444,10 @@ static int walk_stage(gcs_ctx* c, const gcs_params* p, const WalkEpilogue& ep) {
     return check_launch(c, "walk");
 }
 
-static int run_stage(gcs_ctx* c, const gcs_params* p, int stage) {
+// gather_beside_build: the gather runs on the side stream while the build
+// runs on the context stream (set when both stages run in one call; the
+// build stage then joins the side stream, so later stages see both).
+static int run_stage(gcs_ctx* c, const gcs_params* p, int stage, bool gather_beside_build = false) {
     cudaStream_t st = c->stream;
     const Layout L = layout_of(c);
     const int passes = kKeyPasses + seg_passes(c->nseg);
@@ -468,13 +479,27 @@ static int run_stage(gcs_ctx* c, const gcs_params* p, int stage) {
             c->sorted_buf = passes & 1;
             return check_launch(c, "sort");
         }
-        case GCS_STAGE_GATHER:
+        case GCS_STAGE_GATHER: {
+            cudaStream_t gs = st;
+            if (gather_beside_build && ensure_part_stream(c) == GCS_OK &&
+                cudaEventRecord(c->gather_fork, st) == cudaSuccess &&
+                cudaStreamWaitEvent(c->part_stream, c->gather_fork, 0) == cudaSuccess)
+                gs = c->part_stream;
             launch_gather(c->idx[c->sorted_buf], c->pos[c->cur], c->vel[c->cur], c->pos[c->cur ^ 1],
-                          c->vel[c->cur ^ 1], c->n, st);
+                          c->vel[c->cur ^ 1], c->n, gs);
+            if (gs != st) {
+                GCS_CUDA(c, cudaEventRecord(c->gather_join, gs));
+                c->gather_pending = true;
+            }
             c->cur ^= 1;
             return check_launch(c, "gather");
+        }
         case GCS_STAGE_BUILD:
             launch_build(L, c->keys[c->sorted_buf], c->tr, c->bd, c->leaf_parent, c->status, st);
+            if (c->gather_pending) {  // later stages read the gathered records
+                GCS_CUDA(c, cudaStreamWaitEvent(st, c->gather_join, 0));
+                c->gather_pending = false;
+            }
             return check_launch(c, "build");
         case GCS_STAGE_AGGREGATE: {
             const WalkNodeParams wnp = walk_node_params(c, p);
@@ -512,8 +537,9 @@ static int run_stages(gcs_ctx* c, const gcs_params* p, int first, int last) {
         c->last_error = "no particles";
         return GCS_ERR_STATE;
     }
+    const bool gather_beside_build = first <= GCS_STAGE_GATHER && last >= GCS_STAGE_BUILD;
     for (int s = first; s <= last; ++s) {
-        rc = run_stage(c, p, s);
+        rc = run_stage(c, p, s, gather_beside_build);
         if (rc) return rc;
     }
     return GCS_OK;
@@ -906,7 +932,7 @@ int gcs_download_playback(gcs_ctx* c, PlaybackStar* host, int64_t offset, int64_
 static int build_step_graphs(gcs_ctx* c, const gcs_params* p) {
     drop_graphs(c);
     const int cur0 = c->cur;
-    int rc = partitioned(c) ? ensure_part_stream(c) : GCS_OK;
+    int rc = ensure_part_stream(c);  // created outside the capture
     if (rc) return rc;
     for (int k = 0; k < 2 && !rc; ++k) {
         const int parity = cur0 ^ k;
@@ -1349,6 +1375,14 @@ int gcs_walk_stack_peak(gcs_ctx* c, int64_t out[2]) {
     GCS_CUDA(c, cudaStreamSynchronize(c->stream));
     out[0] = (int64_t)peak;
     out[1] = kWalkGlobalStack;
+    return GCS_OK;
+}
+
+int gcs_walk_lane_use(gcs_ctx* c, uint64_t out[8]) {
+    if (!c || !out) return GCS_ERR_ARG;
+    cudaSetDevice(c->device);
+    GCS_CUDA(c, cudaMemcpyAsync(out, c->counts + 9, 8 * sizeof(uint64_t), cudaMemcpyDeviceToHost, c->stream));
+    GCS_CUDA(c, cudaStreamSynchronize(c->stream));
     return GCS_OK;
 }
 

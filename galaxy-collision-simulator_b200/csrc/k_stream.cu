@@ -203,6 +203,7 @@ __global__ void gather_kernel(const uint32_t* __restrict__ idx, const float4* __
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
         const uint32_t s = __ldg(idx + i);
+        if ((int64_t)s >= n) continue;  // only after a sort that timed out (in the status word)
         pos_out[i] = __ldg(pos_in + s);
         vel_out[i] = __ldg(vel_in + s);
     }

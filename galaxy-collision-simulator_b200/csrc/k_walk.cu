@@ -197,7 +197,16 @@ struct WarpCount {
     uint32_t rounds, spills;      // pop rounds, stack spills to global memory
     uint32_t all_open, all_take;  // nodes classified open / take by the box test
     uint32_t peak;                // deepest stack (shared top + global bottom), entries
+    // lane use: evaluated rows (one node or source for every target slot of
+    // the warp) by kind, and the target slots each kind served
+    uint32_t r_list, r_full, r_part, r_mixed;  // take list, full-mask take, other take, mixed
+    uint32_t l_part, l_mixed, l_accept, l_src;  // lanes in masks; mixed: lanes accepting; sources
 };
+
+// Sum over the warp of popc(m) where `in` holds.
+__device__ __forceinline__ uint32_t warp_popc_sum(bool in, uint32_t m) {
+    return (uint32_t)__reduce_add_sync(0xFFFFFFFFu, in ? (uint32_t)__popc(m) : 0u);
+}
 
 // Two evaluation entries for one target, packed (sm_100 f32x2): d = c - x
 // and the softened d2 of both.  Each element is rounded exactly as the
@@ -291,7 +300,14 @@ __device__ __forceinline__ void flush_sources(WarpSmem<H, T>& W, int nsrc, int l
             if (kCount) A[t].n_part += (use0 ? 1u : 0u) + (use1 ? 1u : 0u);
         }
     }
-    if (kCount) WC.w_src += (uint32_t)nsrc;
+    if (kCount) {
+        WC.w_src += (uint32_t)nsrc;
+        for (int e0 = 0; e0 < nsrc; e0 += 32) {
+            const int e = e0 + lane;
+#pragma unroll
+            for (int t = 0; t < T; ++t) WC.l_src += warp_popc_sum(e < nsrc, e < nsrc ? W.srcm[t][e] : 0u);
+        }
+    }
     __syncwarp();
 }
 
@@ -376,6 +392,8 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
         const int seg_n = (int)__ldg(L.seg_off + s + 1) - off;
         WarpCount WC;
         WC.w_node = WC.w_src = WC.rounds = WC.spills = WC.all_open = WC.all_take = WC.peak = 0u;
+        WC.r_list = WC.r_full = WC.r_part = WC.r_mixed = 0u;
+        WC.l_part = WC.l_mixed = WC.l_accept = WC.l_src = 0u;
         int nsrc = 0;
 
         if (seg_n >= 2) {
@@ -414,6 +432,7 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                         if (valid[t]) A[t].n_mono += (uint32_t)fm.x;
                     WC.w_node += (uint32_t)fm.x;
                     WC.all_take += (uint32_t)fm.x;
+                    WC.r_list += (uint32_t)fm.x;
                 }
                 const int32_t* sl = fr.src + (size_t)grp.super * kSuperSrcCap;
                 for (int base = 0; base < fm.y; base += kSrcCap) {
@@ -549,6 +568,17 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                     WC.rounds += 1u;
                     WC.all_open += (uint32_t)(b - n_full - n_take - n_mixed);
                     WC.all_take += (uint32_t)(n_full + n_take);
+                    WC.r_full += (uint32_t)n_full;
+                    WC.r_part += (uint32_t)n_take;
+                    WC.r_mixed += (uint32_t)n_mixed;
+#pragma unroll
+                    for (int h = 0; h < H; ++h) {
+#pragma unroll
+                        for (int t = 0; t < T; ++t) {
+                            WC.l_part += warp_popc_sum(cls[h] == kClassTake, my_mask[h][t]);
+                            WC.l_mixed += warp_popc_sum(cls[h] == kClassMixed, my_mask[h][t]);
+                        }
+                    }
                 }
                 // 3a. nodes every live target accepts: monopole terms, two
                 // nodes per packed evaluation, no masks
@@ -596,7 +626,11 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                         const bool act0 = (mk.x & lane_bit) != 0u, act1 = (mk.y & lane_bit) != 0u;
                         const bool take0 = w2q.x < lim.x, take1 = w2q.y < lim.y;
                         pair_add<kPot>(A[t], d, zm, act0 && take0, act1 && take1);
-                        if (kCount) A[t].n_mono += (act0 && take0 ? 1u : 0u) + (act1 && take1 ? 1u : 0u);
+                        if (kCount) {
+                            A[t].n_mono += (act0 && take0 ? 1u : 0u) + (act1 && take1 ? 1u : 0u);
+                            WC.l_accept += (uint32_t)(__popc(__ballot_sync(kFull, act0 && take0)) +
+                                                      __popc(__ballot_sync(kFull, act1 && take1)));
+                        }
                         const uint32_t om0 = __ballot_sync(kFull, act0 && !take0);
                         const uint32_t om1 = __ballot_sync(kFull, act1 && !take1);
                         if (lane == 0) W.pnopen[t][q] = make_uint2(om0, om1);
@@ -769,6 +803,10 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                 atomicAdd(counts + 6, (unsigned long long)WC.all_open);
                 atomicAdd(counts + 7, (unsigned long long)WC.all_take);
                 atomicMax(counts + 8, (unsigned long long)WC.peak);
+                const uint32_t lu[8] = {WC.r_list, WC.r_full, WC.r_part, WC.r_mixed,
+                                        WC.l_part, WC.l_mixed, WC.l_accept, WC.l_src};
+#pragma unroll
+                for (int k = 0; k < 8; ++k) atomicAdd(counts + 9 + k, (unsigned long long)lu[k]);
             }
         }
         __syncwarp();

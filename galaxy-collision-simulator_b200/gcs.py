@@ -123,6 +123,7 @@ def lib() -> C.CDLL:
                                              C.POINTER(C.c_double)]),
         "gcs_count_interactions": (C.c_int, [P, C.POINTER(Params), C.POINTER(C.c_uint64)]),
         "gcs_walk_stack_peak": (C.c_int, [P, C.POINTER(C.c_int64)]),
+        "gcs_walk_lane_use": (C.c_int, [P, C.POINTER(C.c_uint64)]),
         "gcs_autotune": (C.c_int, [P, C.POINTER(Params), C.POINTER(C.c_double)]),
         "gcs_set_group_width": (C.c_int, [P, i32]),
         "gcs_set_walk_frontier": (C.c_int, [P, i32]),
@@ -396,6 +397,15 @@ class Context:
         self.check(self.L.gcs_count_interactions(self._h, C.byref(p), out))
         r = tuple(int(x) for x in out)
         return r if warp_evals else r[:2]
+
+    def walk_lane_use(self) -> dict:
+        """Rows the last count_interactions evaluated by kind and the lanes
+        (targets) they served; see gcs_walk_lane_use."""
+        out = (C.c_uint64 * 8)()
+        self.check(self.L.gcs_walk_lane_use(self._h, out))
+        keys = ("rows_take_list", "rows_take_full", "rows_take_partial", "rows_mixed",
+                "lanes_take_partial", "lanes_mixed", "lanes_mixed_accepting", "lanes_source")
+        return dict(zip(keys, (int(x) for x in out)))
 
     def walk_stack_peak(self):
         """(deepest walk stack of the last count_interactions in entries,

@@ -307,6 +307,17 @@ int gcs_count_interactions(gcs_ctx* ctx, const gcs_params* p, uint64_t out[8]);
  * context stream.  No counterpart in the reference, whose walk keeps a fixed
  * 256-entry local stack per thread (cuda_engine.cu:106). */
 int gcs_walk_stack_peak(gcs_ctx* ctx, int64_t out[2]);
+/* Lane use of the last gcs_count_interactions.  The walk evaluates rows: one
+ * node or particle source for every target slot of a walk warp at once (32
+ * slots, 64 for groups wider than 32), each target keeping or discarding its
+ * term.  out[0..3]: rows of the super-group take lists, of take nodes holding
+ * every live target, of other take nodes, of mixed nodes (each target
+ * decides); out[4]: targets in the masks of the other take nodes; out[5]:
+ * targets in the masks of mixed nodes; out[6]: of those, the targets that
+ * accepted the node as a monopole; out[7]: targets in the masks of particle
+ * sources (their rows are gcs_count_interactions' out[3]).  Synchronises the context stream.  No counterpart in the
+ * reference, whose walk gives each target its own thread. */
+int gcs_walk_lane_use(gcs_ctx* ctx, uint64_t out[8]);
 /* Autotuner: times the walk on the current state for leaf sizes
  * {1,2,4,8,16,32} from p->tune_leaf_min up to p->leaf_size (the caller's
  * "leaf <= L"; leaf size 2 gives exactly the reference's terms, sizes >= 3

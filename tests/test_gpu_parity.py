@@ -221,6 +221,18 @@ def test_walk_frontier_keeps_every_targets_terms(gcs_mod, oracle_mod, width, the
             peak, global_cap = ctx.walk_stack_peak()
             # the deepest stack a walk warp held fits the shared top plus the global bottom
             assert 0 < peak <= global_cap + 512, (frontier, peak)
+            # every monopole term came from a row: full rows serve at most 32
+            # lanes, other take rows and mixed rows the lanes counted for them
+            lu = ctx.walk_lane_use()
+            n_mono, n_part = want
+            slots = 64 if width > 32 else 32  # target slots of a walk warp
+            some = lu["lanes_take_partial"] + lu["lanes_mixed_accepting"]
+            assert some <= n_mono <= some + slots * (lu["rows_take_list"] + lu["rows_take_full"]), lu
+            assert lu["lanes_mixed_accepting"] <= lu["lanes_mixed"] <= slots * lu["rows_mixed"], lu
+            assert lu["lanes_take_partial"] <= slots * lu["rows_take_partial"], lu
+            assert n_part <= lu["lanes_source"], lu
+            if not frontier:
+                assert lu["rows_take_list"] == 0, lu
         assert ctx.device_status() == 0
 
 
