@@ -144,6 +144,7 @@ struct WarpSmem {
     using Entry = typename EntryOf<T>::type;
     static constexpr int kBatch = 32 * H;
     static constexpr int kPairs = kBatch / 2 + 2;  // three padded lists
+    static_assert(2 * kPairs >= kBatch, "a source descriptor per popped node fits sdesc and pmask");
     // A round starts with top <= kSpillAbove (or < kBatch before a refill of
     // <= kSpillCount) and pushes <= 2 * batch; one spill of kSpillCount
     // brings top back to <= kSpillAbove.
@@ -152,8 +153,16 @@ struct WarpSmem {
     static_assert(kSpillAbove >= kSpillCount && kBatch <= kSpillCount, "stack sizing");
     static_assert(2 * kBatch + kSpillCount - 1 <= kStackCap, "refill then push must fit");
     Entry stk[kStackCap];           // node, lane masks
-    float4 pxy[kPairs];             // x0 x1 y0 y1 of the centres of mass of slots 2q, 2q+1
-    float4 pzm[kPairs];             // z0 z1 Gm0 Gm1
+    union {
+        struct {
+            float4 pxy[kPairs];     // x0 x1 y0 y1 of the centres of mass of slots 2q, 2q+1
+            float4 pzm[kPairs];     // z0 z1 Gm0 Gm1
+        };
+        // after a round's evaluation: one descriptor per node with particle
+        // sources (first source in the round, its two child codes), in source
+        // order; the lane masks go to pmask
+        int4 sdesc[2 * kPairs];
+    };
     float2 pw2[kPairs];             // width^2 of both slots
     uint2 pmask[T][kPairs];         // lane masks of both slots, per target slot
     uint2 pnopen[T][kPairs];        // opening lanes of both slots (mixed nodes)
@@ -683,30 +692,62 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                 // list, flushing between windows
                 const int src_at = (int)(excl & 0xFFFFu);
                 const int add = (int)(total & 0xFFFFu);
-                for (int base = 0; base < add;) {
-                    if (nsrc == kSrcCap) {
-                        flush_sources<H, T, kPot, kCount>(W, nsrc, lane, lane_bit, pos, G, X, e2, leaf_thr, A, WC);
-                        nsrc = 0;
-                    }
-                    const int window = min(kSrcCap - nsrc, add - base);
-                    int first = src_at;  // this lane's first source index in the round
+                if (add > 0) {
+                    // one descriptor per node with sources, lane-major like
+                    // the sources themselves: the lanes before this one hold
+                    // descriptors [0, before)
+                    int before = 0, n_desc = 0;
 #pragma unroll
                     for (int h = 0; h < H; ++h) {
-                        const int j0 = max(first, base), j1 = min(first + n_src[h], base + window);
-                        for (int j = j0; j < j1; ++j) {
-                            const int r = j - first;  // r-th source of node h
-                            int particle;
-                            if (code_b[h] >= kWalkBucketTag) particle = code_a[h] + r;
-                            else particle = (r == 0 && code_a[h] < 0) ? ~code_a[h] : ~code_b[h];
+                        const uint32_t bh = __ballot_sync(kFull, n_src[h] > 0);
+                        before += __popc(bh & lt);
+                        n_desc += __popc(bh);
+                    }
+                    {
+                        int d = before, first = src_at;
+#pragma unroll
+                        for (int h = 0; h < H; ++h) {
+                            if (n_src[h] > 0) {
+                                W.sdesc[d] = make_int4(first, code_a[h], code_b[h], 0);
+#pragma unroll
+                                for (int t = 0; t < T; ++t)
+                                    reinterpret_cast<uint32_t*>(W.pmask[t])[d] = my_open[h][t];
+                                ++d;
+                            }
+                            first += n_src[h];
+                        }
+                    }
+                    __syncwarp();
+                    // the round's sources [0, add), appended in windows that
+                    // fit the list (flushing between windows), one per lane
+                    for (int base = 0; base < add;) {
+                        if (nsrc == kSrcCap) {
+                            flush_sources<H, T, kPot, kCount>(W, nsrc, lane, lane_bit, pos, G, X, e2, leaf_thr, A,
+                                                              WC);
+                            nsrc = 0;
+                        }
+                        const int window = min(kSrcCap - nsrc, add - base);
+                        for (int j = base + lane; j < base + window; j += 32) {
+                            // the last descriptor starting at or before j
+                            int lo = 0, hi = n_desc - 1;
+                            while (lo < hi) {
+                                const int mid = (lo + hi + 1) >> 1;
+                                if (W.sdesc[mid].x <= j) lo = mid;
+                                else hi = mid - 1;
+                            }
+                            const int4 e = W.sdesc[lo];
+                            const int r = j - e.x;  // r-th source of that node
+                            const int particle = e.z >= kWalkBucketTag ? e.y + r
+                                               : ((r == 0 && e.y < 0) ? ~e.y : ~e.z);
                             const int at = nsrc + (j - base);
                             W.srcp[at] = particle;
 #pragma unroll
-                            for (int t = 0; t < T; ++t) W.srcm[t][at] = my_open[h][t];
+                            for (int t = 0; t < T; ++t)
+                                W.srcm[t][at] = reinterpret_cast<const uint32_t*>(W.pmask[t])[lo];
                         }
-                        first += n_src[h];
+                        nsrc += window;
+                        base += window;
                     }
-                    nsrc += window;
-                    base += window;
                 }
                 __syncwarp();
                 if (nsrc >= 32) {
