@@ -900,7 +900,9 @@ def main():
 
     stars = gcs.collision_equal(*counts_for(args.n), seed=rank)
     n = len(stars)
-    stream = torch.cuda.current_stream()
+    # a stream of its own: the timed steps run as the library's captured CUDA
+    # graphs (gcs_set_graphs), which need a non-default stream
+    stream = torch.cuda.Stream(device=local)
     ctx = gcs.Context(n, device=local)
     ctx.set_stream(stream.cuda_stream)
     ctx.upload(stars)
@@ -932,6 +934,18 @@ def main():
     lane_use["useful_lane_fraction"] = (n_mono + n_part) / (float(slots) * rows) if rows else None
     ctx.upload(stars)
 
+    # each timed step is one graph launch of the whole step; the library
+    # records a pair of events around the walk inside the graph (event-record
+    # nodes pointed at step k's pair before its launch), so the walk's own
+    # time is measured in the same timed region
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    wev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for a, b in wev:  # create the events
+        a.record(stream)
+        b.record(stream)
+    ctx.set_graphs(True)
+    ctx.set_walk_events(wev[0][0], wev[0][1])
     for _ in range(args.warmup):
         ctx.step(p)
     torch.cuda.synchronize()
@@ -940,20 +954,17 @@ def main():
 
     sampler = ClockSampler(local)
     sampler.start()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    wev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     ev0.record(stream)
     for k in range(args.steps):
-        ctx.run_stages(p, gcs.STAGE_BOUNDS, gcs.STAGE_AGGREGATE)
-        wev[k][0].record(stream)
-        ctx.run_stages(p, gcs.STAGE_WALK, gcs.STAGE_WALK)
-        wev[k][1].record(stream)
-        ctx.run_stages(p, gcs.STAGE_INTEGRATE, gcs.STAGE_INTEGRATE)
+        ctx.set_walk_events(wev[k][0], wev[k][1])
+        ctx.step(p)
     ev1.record(stream)
     torch.cuda.synchronize()
     barrier()
     clocks = sampler.stop()
+    graph_builds = ctx.graph_builds
+    ctx.set_walk_events(None, None)
+    ctx.set_graphs(False)
     status = ctx.device_status()
     if status:
         raise RuntimeError("device status word 0x%x after the timed steps" % status)
@@ -997,14 +1008,18 @@ def main():
                 "walk_stack_peak": stack_peak, "walk_stack_global_per_warp": stack_global,
                 "walk_lane_use": lane_use}
     passes = 8
-    launches_per_step = 2 + 1 + passes + 1 + 1 + 1 + 1 + 1
+    # bounds + decode, encode, the sort passes, gather, build, aggregate,
+    # partition, frontier, walk, integrate
+    launches_per_step = 2 + 1 + passes + 1 + 1 + 1 + 3 + 1
     line = {"metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded two-galaxy initial conditions, seed = rank)",
             "config": bench_config(n, world),
             "settings": {"leaf_size": p.leaf_size, "walk_batch": p.walk_batch, "group_width": ctx.group_width,
-                         "autotuned": tuned, "com": "fp64 sums", "bounds": "device, per step"},
+                         "autotuned": tuned, "com": "fp64 sums", "bounds": "device, per step",
+                         "step": "one CUDA graph launch per step (gcs_set_graphs), graph captures: %d"
+                                 % graph_builds},
             "e2e": e2e, "roofline": roofline, "clocks": clocks, "gpu_launches": launches_per_step * args.steps,
             "device_status": status}
     if rank == 0 and world == 1:

@@ -136,6 +136,13 @@ struct gcs_ctx {
     cudaStream_t graph_stream = nullptr;
     cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
     int graph_builds = 0;
+    // caller's events recorded around the walk stage (gcs_set_walk_events);
+    // in a captured step they are event-record nodes, pointed at the events
+    // set now before each launch
+    cudaEvent_t walk_ev[2] = {nullptr, nullptr};
+    cudaGraph_t graph[2] = {nullptr, nullptr};  // kept: their nodes address the exec graphs' nodes
+    cudaGraphNode_t walk_ev_node[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [parity][start, end]
+    cudaEvent_t walk_ev_bound[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
 
     std::string last_error;
 };
@@ -221,7 +228,26 @@ void drop_graphs(gcs_ctx* c) {
         if (g) cudaGraphExecDestroy(g);
         g = nullptr;
     }
+    for (auto& g : c->graph) {
+        if (g) cudaGraphDestroy(g);
+        g = nullptr;
+    }
+    for (int k = 0; k < 2; ++k)
+        for (int e = 0; e < 2; ++e) {
+            c->walk_ev_node[k][e] = nullptr;
+            c->walk_ev_bound[k][e] = nullptr;
+        }
     c->graphs_valid = false;
+}
+
+// Record a caller's event on the context stream; under stream capture it
+// becomes an event-record node of the graph.
+cudaError_t record_event(cudaEvent_t ev, cudaStream_t st) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    const cudaError_t e = cudaStreamIsCapturing(st, &cs);
+    if (e != cudaSuccess) return e;
+    return cs == cudaStreamCaptureStatusActive ? cudaEventRecordWithFlags(ev, st, cudaEventRecordExternal)
+                                               : cudaEventRecord(ev, st);
 }
 
 void free_all(gcs_ctx* c) {
@@ -511,8 +537,13 @@ static int run_stage(gcs_ctx* c, const gcs_params* p, int stage, bool gather_bes
             c->wn_L = wnp.leaf_size;
             return check_launch(c, "aggregate");
         }
-        case GCS_STAGE_WALK:
-            return walk_stage(c, p, WalkEpilogue());
+        case GCS_STAGE_WALK: {
+            if (c->walk_ev[0]) GCS_CUDA(c, record_event(c->walk_ev[0], st));
+            const int rc = walk_stage(c, p, WalkEpilogue());
+            if (rc) return rc;
+            if (c->walk_ev[1]) GCS_CUDA(c, record_event(c->walk_ev[1], st));
+            return GCS_OK;
+        }
         case GCS_STAGE_INTEGRATE: {
             const int64_t f = range_first(c);
             launch_integrate(c->pos[c->cur] + f, c->vel[c->cur] + f, c->acc + f, p->dt, p->recolor, range_count(c),
@@ -956,7 +987,34 @@ static int build_step_graphs(gcs_ctx* c, const gcs_params* p) {
                 rc = GCS_ERR_CUDA;
             }
         }
-        if (graph) cudaGraphDestroy(graph);
+        if (!rc && (c->walk_ev[0] || c->walk_ev[1])) {
+            // the event-record nodes of the caller's walk events
+            size_t count = 0;
+            if (cudaGraphGetNodes(graph, nullptr, &count) == cudaSuccess && count > 0) {
+                std::vector<cudaGraphNode_t> nodes(count);
+                if (cudaGraphGetNodes(graph, nodes.data(), &count) == cudaSuccess) {
+                    for (size_t i = 0; i < count; ++i) {
+                        cudaGraphNodeType type;
+                        cudaEvent_t ev = nullptr;
+                        if (cudaGraphNodeGetType(nodes[i], &type) != cudaSuccess ||
+                            type != cudaGraphNodeTypeEventRecord ||
+                            cudaGraphEventRecordNodeGetEvent(nodes[i], &ev) != cudaSuccess)
+                            continue;
+                        for (int e = 0; e < 2; ++e)
+                            if (ev && ev == c->walk_ev[e]) {
+                                c->walk_ev_node[parity][e] = nodes[i];
+                                c->walk_ev_bound[parity][e] = ev;
+                            }
+                    }
+                }
+            }
+            for (int e = 0; e < 2; ++e)
+                if (c->walk_ev[e] && !c->walk_ev_node[parity][e]) {
+                    c->last_error = "walk event node missing from the captured step";
+                    rc = GCS_ERR_CUDA;
+                }
+        }
+        c->graph[parity] = graph;  // destroyed with the exec graphs
     }
     c->cur = cur0;
     if (rc) {
@@ -986,9 +1044,28 @@ int gcs_step(gcs_ctx* c, const gcs_params* p) {
         if (rc) return rc;
     }
     cudaSetDevice(c->device);
+    for (int e = 0; e < 2; ++e) {
+        // point the graph's walk-event nodes at the events set now
+        cudaGraphNode_t node = c->walk_ev_node[c->cur][e];
+        if (node && c->walk_ev[e] && c->walk_ev_bound[c->cur][e] != c->walk_ev[e]) {
+            GCS_CUDA(c, cudaGraphExecEventRecordNodeSetEvent(c->graph_exec[c->cur], node, c->walk_ev[e]));
+            c->walk_ev_bound[c->cur][e] = c->walk_ev[e];
+        }
+    }
     GCS_CUDA(c, cudaGraphLaunch(c->graph_exec[c->cur], c->stream));
     c->cur ^= 1;  // the captured gather flipped the arrays
     c->sorted_buf = (kKeyPasses + seg_passes(c->nseg)) & 1;
+    return GCS_OK;
+}
+
+int gcs_set_walk_events(gcs_ctx* c, void* start, void* end) {
+    if (!c) return GCS_ERR_ARG;
+    cudaEvent_t ev[2] = {static_cast<cudaEvent_t>(start), static_cast<cudaEvent_t>(end)};
+    // graphs hold event-record nodes only for events present at capture
+    if ((ev[0] != nullptr) != (c->walk_ev[0] != nullptr) || (ev[1] != nullptr) != (c->walk_ev[1] != nullptr))
+        drop_graphs(c);
+    c->walk_ev[0] = ev[0];
+    c->walk_ev[1] = ev[1];
     return GCS_OK;
 }
 

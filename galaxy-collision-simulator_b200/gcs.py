@@ -130,6 +130,7 @@ def lib() -> C.CDLL:
         "gcs_group_width": (i32, [P]),
         "gcs_sort_pairs_static": (C.c_int, [P, P, P, P, i64, P, P]),
         "gcs_set_graphs": (C.c_int, [P, i32]),
+        "gcs_set_walk_events": (C.c_int, [P, C.c_void_p, C.c_void_p]),
         "gcs_graph_builds": (i32, [P]),
         "gcs_relayout": (C.c_int, [P, i32, C.POINTER(i64), C.POINTER(i32)]),
         "gcs_segment_offset": (i64, [P, i32]),
@@ -374,6 +375,19 @@ class Context:
 
     def set_graphs(self, enable: bool) -> None:
         self.check(self.L.gcs_set_graphs(self._h, int(enable)))
+
+    def set_walk_events(self, start, end) -> None:
+        """Record two CUDA events (torch.cuda.Event, a raw cudaEvent_t as an
+        int, or None) around every walk stage from now on, also inside
+        graph-captured steps; see gcs_set_walk_events."""
+        def handle(e):
+            if e is None:
+                return None
+            h = getattr(e, "cuda_event", e)
+            if not h:
+                raise ValueError("the event has no CUDA event yet (record it once first)")
+            return C.c_void_p(int(h))
+        self.check(self.L.gcs_set_walk_events(self._h, handle(start), handle(end)))
 
     @property
     def graph_builds(self) -> int:

@@ -166,6 +166,15 @@ int gcs_step(gcs_ctx* ctx, const gcs_params* p);
  * arrays) and recaptures only when the parameters, the segment layout, the
  * group width or the stream change.  Needs a non-default stream. */
 int gcs_set_graphs(gcs_ctx* ctx, int32_t enable);
+/* Timing hooks: `start` and `end` (cudaEvent_t, or NULL) are recorded on the
+ * context stream right before and after every walk stage from now on, in
+ * eager steps and inside graph-captured steps alike (there they are
+ * event-record nodes; a gcs_step after a change of events points those nodes
+ * at the new events before it launches, so each step can be timed with its
+ * own pair).  Setting or clearing an event recaptures the graphs at the next
+ * gcs_step; replacing one by another does not.  No counterpart in the
+ * reference. */
+int gcs_set_walk_events(gcs_ctx* ctx, void* start, void* end);
 /* How many times the step graphs have been captured on this context. */
 int32_t gcs_graph_builds(const gcs_ctx* ctx);
 /* One step with every particle's stepped Star (sorted order) written to

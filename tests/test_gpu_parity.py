@@ -279,6 +279,44 @@ def test_group_width_and_autotune(gcs_mod, oracle_mod, stars):
         assert ctx.device_status() == 0
 
 
+def test_walk_events_time_eager_and_graph_steps(gcs_mod, stars):
+    """Caller events around the walk stage: recorded in eager steps and
+    inside captured steps, re-pointed per step without a new capture, and
+    the state stays byte-identical to steps without events."""
+    import torch
+    gcs = gcs_mod
+    s = torch.cuda.Stream()
+    p = _params(gcs, leaf_size=4, com_fp64=1)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(6)]
+    for a, b in evs:
+        a.record(s)
+        b.record(s)
+    with _ctx(gcs, stars) as plain, _ctx(gcs, stars) as timed:
+        plain.set_stream(s.cuda_stream)
+        timed.set_stream(s.cuda_stream)
+        for k in range(2):  # eager
+            timed.set_walk_events(*evs[k])
+            timed.step(p)
+            plain.step(p)
+        plain.set_graphs(True)
+        timed.set_graphs(True)
+        for k in range(2, 6):  # captured once, events re-pointed each step
+            timed.set_walk_events(*evs[k])
+            timed.step(p)
+            plain.step(p)
+        torch.cuda.synchronize()
+        assert timed.graph_builds == 1
+        walk = [a.elapsed_time(b) for a, b in evs]
+        assert all(w > 0.0 for w in walk), walk
+        assert plain.download().tobytes() == timed.download().tobytes()
+        timed.set_walk_events(None, None)  # presence changes: captured again
+        timed.step(p)
+        plain.step(p)
+        assert timed.graph_builds == 2
+        assert plain.download().tobytes() == timed.download().tobytes()
+        assert timed.device_status() == 0
+
+
 def test_graph_steps_match_eager_steps(gcs_mod, stars):
     """The captured step is the eager step: byte-identical state after
     several steps, one capture per parameter set."""
