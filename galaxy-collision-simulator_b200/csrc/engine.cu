@@ -135,6 +135,7 @@ struct gcs_ctx {
     gcs_params graph_params;
     cudaStream_t graph_stream = nullptr;
     cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
+    int graph_after[2] = {1, 0};  // parity of the particle arrays after the graph of each parity
     int graph_builds = 0;
     // caller's events recorded around the walk stage (gcs_set_walk_events);
     // in a captured step they are event-record nodes, pointed at the events
@@ -473,7 +474,12 @@ static int walk_stage(gcs_ctx* c, const gcs_params* p, const WalkEpilogue& ep) {
 // gather_beside_build: the gather runs on the side stream while the build
 // runs on the context stream (set when both stages run in one call; the
 // build stage then joins the side stream, so later stages see both).
-static int run_stage(gcs_ctx* c, const gcs_params* p, int stage, bool gather_beside_build = false) {
+// kick_in_walk: the walk's warps apply the kick/drift to their groups as they
+// finish them (out of place, into the other particle arrays) and the
+// integrate stage has nothing left to do (set when both stages run in one
+// call over all particles).
+static int run_stage(gcs_ctx* c, const gcs_params* p, int stage, bool gather_beside_build = false,
+                     bool kick_in_walk = false) {
     cudaStream_t st = c->stream;
     const Layout L = layout_of(c);
     const int passes = kKeyPasses + seg_passes(c->nseg);
@@ -539,12 +545,22 @@ static int run_stage(gcs_ctx* c, const gcs_params* p, int stage, bool gather_bes
         }
         case GCS_STAGE_WALK: {
             if (c->walk_ev[0]) GCS_CUDA(c, record_event(c->walk_ev[0], st));
-            const int rc = walk_stage(c, p, WalkEpilogue());
+            WalkEpilogue ep;
+            if (kick_in_walk) {
+                ep.vel_in = c->vel[c->cur];
+                ep.pos_out = c->pos[c->cur ^ 1];
+                ep.vel_out = c->vel[c->cur ^ 1];
+                ep.dt = p->dt;
+                ep.recolor = p->recolor;
+            }
+            const int rc = walk_stage(c, p, ep);
             if (rc) return rc;
+            if (kick_in_walk) c->cur ^= 1;  // the stepped state is in the other arrays
             if (c->walk_ev[1]) GCS_CUDA(c, record_event(c->walk_ev[1], st));
             return GCS_OK;
         }
         case GCS_STAGE_INTEGRATE: {
+            if (kick_in_walk) return GCS_OK;  // the walk applied it
             const int64_t f = range_first(c);
             launch_integrate(c->pos[c->cur] + f, c->vel[c->cur] + f, c->acc + f, p->dt, p->recolor, range_count(c),
                              st);
@@ -569,8 +585,9 @@ static int run_stages(gcs_ctx* c, const gcs_params* p, int first, int last) {
         return GCS_ERR_STATE;
     }
     const bool gather_beside_build = first <= GCS_STAGE_GATHER && last >= GCS_STAGE_BUILD;
+    const bool kick_in_walk = first <= GCS_STAGE_WALK && last >= GCS_STAGE_INTEGRATE && c->range_count < 0;
     for (int s = first; s <= last; ++s) {
-        rc = run_stage(c, p, s, gather_beside_build);
+        rc = run_stage(c, p, s, gather_beside_build, kick_in_walk);
         if (rc) return rc;
     }
     return GCS_OK;
@@ -975,6 +992,7 @@ static int build_step_graphs(gcs_ctx* c, const gcs_params* p) {
             break;
         }
         rc = run_stages(c, p, GCS_STAGE_BOUNDS, GCS_STAGE_INTEGRATE);
+        c->graph_after[parity] = c->cur;
         const cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
         if (!rc && e != cudaSuccess) {
             set_error(c, "cudaStreamEndCapture", e);
@@ -1053,7 +1071,7 @@ int gcs_step(gcs_ctx* c, const gcs_params* p) {
         }
     }
     GCS_CUDA(c, cudaGraphLaunch(c->graph_exec[c->cur], c->stream));
-    c->cur ^= 1;  // the captured gather flipped the arrays
+    c->cur = c->graph_after[c->cur];  // the flips the captured step made (gather, kick/drift in the walk)
     c->sorted_buf = (kKeyPasses + seg_passes(c->nseg)) & 1;
     return GCS_OK;
 }

@@ -53,7 +53,7 @@
 //
 // With an epilogue (WalkEpilogue), a warp that has written its group's
 // accelerations also applies the step's kick/drift to those particles, out of
-// place, and writes their Star records; the warp that completes a chunk of
+// place, and writes their Star records (when given); the warp that completes a chunk of
 // groups raises that chunk's flag in mapped host memory (chunks are large
 // over the groups handed out early and small over the last ones, which are
 // all in flight together at the end).  The host copies
@@ -798,7 +798,7 @@ walk_kernel(Layout L, WalkParams wp, const float4* __restrict__ pos,
                 kick_drift(p, v, a, ep.dt, ep.recolor);
                 ep.pos_out[i] = p;
                 ep.vel_out[i] = v;
-                store_star(ep.stars, i, p, v);
+                if (ep.stars) store_star(ep.stars, i, p, v);
             }
         }
         if (ep.vel_in && ep.host_flags) {
