@@ -1009,8 +1009,8 @@ def main():
                 "walk_lane_use": lane_use}
     passes = 8
     # bounds + decode, encode, the sort passes, gather, build, aggregate,
-    # partition, frontier, walk, integrate
-    launches_per_step = 2 + 1 + passes + 1 + 1 + 1 + 3 + 1
+    # partition, frontier, walk (which also applies the kick/drift)
+    launches_per_step = 2 + 1 + passes + 1 + 1 + 1 + 3
     line = {"metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
