@@ -279,6 +279,30 @@ def test_group_width_and_autotune(gcs_mod, oracle_mod, stars):
         assert ctx.device_status() == 0
 
 
+@pytest.mark.parametrize("width", [32, 64])
+def test_kick_in_walk_equals_integrate_launch(gcs_mod, width):
+    """A full step applies the kick/drift in the walk's epilogue; running the
+    walk and the integrate stage in separate calls launches integrate_kernel.
+    Both give the same bytes, over uneven segments (a 1-particle one too)."""
+    gcs = gcs_mod
+    a = small_collision(1500, 400, 211, seed=51)
+    b = small_collision(300, 90, 17, seed=52)
+    one = small_collision(64, 16, 8, seed=53)[:1]
+    st = np.concatenate([a, one, b])
+    segs = [len(a), 1, len(b)]
+    p = _params(gcs, leaf_size=4, walk_batch=64, com_fp64=1)
+    with _ctx(gcs, st, segs) as fused, _ctx(gcs, st, segs) as split:
+        fused.set_group_width(width)
+        split.set_group_width(width)
+        for _ in range(3):
+            fused.run_stages(p, gcs.STAGE_BOUNDS, gcs.STAGE_INTEGRATE)
+            split.run_stages(p, gcs.STAGE_BOUNDS, gcs.STAGE_WALK)
+            split.run_stages(p, gcs.STAGE_INTEGRATE, gcs.STAGE_INTEGRATE)
+            assert fused.download().tobytes() == split.download().tobytes()
+            np.testing.assert_array_equal(fused.read(gcs.BUF_ACCEL), split.read(gcs.BUF_ACCEL))
+        assert fused.device_status() == 0 and split.device_status() == 0
+
+
 def test_walk_events_time_eager_and_graph_steps(gcs_mod, stars):
     """Caller events around the walk stage: recorded in eager steps and
     inside captured steps, re-pointed per step without a new capture, and
