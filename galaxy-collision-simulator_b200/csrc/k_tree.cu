@@ -142,15 +142,18 @@ __device__ __forceinline__ ChildData load_child(int c, int n_internal, const flo
     return r;
 }
 
-constexpr int kAggThreads = 256;
+constexpr uint32_t kFull = 0xFFFFFFFFu;
+constexpr int kAggThreads = 128;     // threads of an aggregation block
+constexpr int kAggRange = 512;       // particles a block owns (its lanes take them as they finish)
+constexpr int kAggBlocksPerSm = 8;
 // FP64 centre-of-mass sums (com_fp64) are kept for the top of the tree:
 // nodes of at least this many particles, where the mass-weighted positions
 // of many particles are summed.  A child below the size (or a particle)
 // enters its parent's sums as the exact double product of its FP32 mass and
-// centre of mass (position).  Block-local nodes hold at most kAggThreads
+// centre of mass (position).  Block-local nodes hold at most kAggRange
 // particles, so they are never FP64 nodes.
 constexpr int kComFp64Min = 1024;
-static_assert(kComFp64Min > kAggThreads, "block-local nodes are never FP64 nodes");
+static_assert(kComFp64Min > kAggRange, "block-local nodes are never FP64 nodes");
 
 // A node finished inside the block, kept in shared memory for its parent.
 struct LocalNode {
@@ -227,81 +230,109 @@ __global__ void walk_nodes_kernel(Layout L, const BvhNodeTraverse* __restrict__ 
     }
 }
 
-// One thread per particle; block b owns particles [256 b, 256 b + 256).  A
-// node whose particle range lies inside its block's range has both children
-// finished by threads of that block: its arrival counter and the finished
-// children live in shared memory and the handshake is block-scoped.  Every
-// other node uses the GPU-scope counter in its build record.  The side a
-// node uses depends only on the node, so both arrivals always meet.
-__global__ void __launch_bounds__(kAggThreads, 4)
-aggregate_kernel(Layout L, const float4* __restrict__ pos,
-                                 BvhNodeTraverse* __restrict__ tr, BvhNodeBuild* __restrict__ bd,
-                                 double4* __restrict__ com64, const int32_t* __restrict__ leaf_parent,
-                                 int com_fp64, WalkNodeParams wnp, uint32_t* __restrict__ status) {
-    __shared__ int sflag[kAggThreads];
-    __shared__ LocalNode snode[kAggThreads];
+// Block b owns particles [kAggRange b, kAggRange (b + 1)).  A node whose
+// particle range lies inside its block's range has both children finished by
+// threads of that block: its arrival counter and the finished children live
+// in shared memory and the handshake is block-scoped.  Every other node uses
+// the GPU-scope counter in its build record.  The side a node uses depends
+// only on the node, so both arrivals always meet.
+//
+// Each lane climbs from one particle at a time: it arrives at the parent of
+// what it has just finished; the first arrival stops, the second computes the
+// parent and climbs on.  A lane whose climb has stopped takes the block's
+// next particle at once (the warp claims particles for all its idle lanes
+// with one shared-memory atomic), so a warp keeps its lanes busy instead of
+// running as long as its longest-climbing lane.  Which lane computes a node
+// does not change its value.
+__global__ void __launch_bounds__(kAggThreads, kAggBlocksPerSm)
+aggregate_kernel(Layout L, const float4* __restrict__ pos, BvhNodeTraverse* __restrict__ tr,
+                 BvhNodeBuild* __restrict__ bd, double4* __restrict__ com64,
+                 const int32_t* __restrict__ leaf_parent, int com_fp64, WalkNodeParams wnp,
+                 uint32_t* __restrict__ status) {
+    __shared__ int sflag[kAggRange];
+    __shared__ LocalNode snode[kAggRange];
+    __shared__ int s_next;  // the block's next unclaimed particle
     const bool fp64 = com_fp64 != 0;
-    const int b0 = blockIdx.x * kAggThreads;
-    sflag[threadIdx.x] = 0;
+    const int lane = threadIdx.x & 31;
+    const uint32_t lt = (1u << lane) - 1u;
+    const int ni = L.n_internal;
+    const int b0 = blockIdx.x * kAggRange;
+    const int b_end = min(b0 + kAggRange, L.n);
+    for (int i = threadIdx.x; i < kAggRange; i += kAggThreads) sflag[i] = 0;
+    if (threadIdx.x == 0) s_next = b0;
     __syncthreads();
-    const int g = b0 + threadIdx.x;
-    if (g >= L.n) return;
-    const int s = L.nseg > 1 ? __ldg(L.seg_id + g) : 0;
-    const int seg_lo = (int)__ldg(L.seg_off + s), seg_hi = (int)__ldg(L.seg_off + s + 1) - 1;
-    // The node this thread has just finished (first the leaf itself) is
-    // carried in registers; at each parent only the sibling is loaded.
-    int from = L.n_internal + g;
-    ChildData mine = load_child(from, L.n_internal, pos, tr, bd, com64, false);
-    int node = __ldg(leaf_parent + g);
-    // Links come from the build launch, so they can be read at any time: the
-    // first node's before the climb, each parent's as soon as the climb is
-    // known to continue to it (overlapping the sibling load and the node's
-    // arithmetic).
-    int cl = -1, cr = -1, up = -1, re = 0;
-    if (node >= 0 && node < L.n_internal) {
-        cl = __ldg(&tr[node].child_left);
-        cr = __ldg(&tr[node].child_right);
-        up = __ldg(&bd[node].parent);
-        re = __ldg(&tr[node].range_end);
-    }
-    int levels = 0;
-    while (node >= 0) {
-        // a valid tree has at most 96 internal levels (strictly increasing
-        // prefix lengths below 96); more means malformed parent links
-        if (++levels > 96 || node >= L.n_internal) {
+    bool have = false;  // this lane is climbing
+    int s = 0, seg_lo = 0, seg_hi = 0, from = 0, node = -1, cl = -1, cr = -1, up = -1, re = 0, levels = 0;
+    ChildData mine;
+    for (;;) {
+        // idle lanes take the block's next particles
+        const uint32_t idle = __ballot_sync(kFull, !have);
+        if (idle) {
+            const int leader = __ffs(idle) - 1;
+            int base = 0;
+            if (lane == leader) base = atomicAdd(&s_next, __popc(idle));
+            base = __shfl_sync(kFull, base, leader);
+            if (!have) {
+                const int g = base + __popc(idle & lt);
+                if (g < b_end) {
+                    s = L.nseg > 1 ? __ldg(L.seg_id + g) : 0;
+                    seg_lo = (int)__ldg(L.seg_off + s);
+                    seg_hi = (int)__ldg(L.seg_off + s + 1) - 1;
+                    from = ni + g;
+                    mine = load_child(from, ni, pos, tr, bd, com64, false);
+                    node = __ldg(leaf_parent + g);
+                    levels = 0;
+                    if (node >= 0 && node < ni) {
+                        cl = __ldg(&tr[node].child_left);
+                        cr = __ldg(&tr[node].child_right);
+                        up = __ldg(&bd[node].parent);
+                        re = __ldg(&tr[node].range_end);
+                    }
+                    have = node >= 0;  // a one-particle segment has no parent
+                }
+            }
+        }
+        if (!__any_sync(kFull, have)) break;
+        if (!have) continue;
+        // one step of this lane's climb: arrive at `node`, the parent of `from`
+        // (a valid tree has at most 96 internal levels: strictly increasing
+        // prefix lengths below 96; more means malformed parent links)
+        if (++levels > 96 || node >= ni) {
             atomicOr(status, GCS_DEV_TREE_MALFORMED);
-            break;
+            have = false;
+            continue;
         }
         const int own = node + s;  // particle index at this end of the node's range
-        const bool local = min(own, re) >= b0 && max(own, re) < b0 + kAggThreads;
+        const bool local = min(own, re) >= b0 && max(own, re) < b0 + kAggRange;
         int old;
         if (local) {
-            // block scope: this thread's writes (shared and global) before
-            // the arrival, the sibling's after it
+            // block scope: this lane's writes (shared and global) before the
+            // arrival, the sibling's after it
             __threadfence_block();
             old = atomicAdd(&sflag[own - b0], 1);
-            if (old == 0) break;
-            __threadfence_block();
+            if (old != 0) __threadfence_block();
         } else if (levels == 1) {
-            // At the leaf level this thread has written nothing, so its
-            // arrival needs no release; it acquires only if it arrives second.
+            // at the leaf level this lane has written nothing for `from`, so
+            // its arrival needs no release; it acquires only if it arrives second
             old = arrive_relaxed(&bd[node].flag);
-            if (old == 0) break;
-            fence_acq_rel();
+            if (old != 0) fence_acq_rel();
         } else {
-            // release: this thread's writes of the child it just finished are
-            // visible to whoever acquires the counter next; acquire: the
-            // second arrival sees the sibling's writes
+            // release: the child this lane just finished is visible to whoever
+            // acquires the counter next; acquire: the second arrival sees the
+            // sibling's writes
             old = arrive_acq_rel(&bd[node].flag);
-            if (old == 0) break;                // first arrival: the sibling finishes
         }
-        if (cl < 0 || cr < 0 || cl >= L.n_internal + L.n || cr >= L.n_internal + L.n ||
-            (cl != from && cr != from)) {
+        if (old == 0) {  // first arrival: the sibling's climb finishes the node
+            have = false;
+            continue;
+        }
+        if (cl < 0 || cr < 0 || cl >= ni + L.n || cr >= ni + L.n || (cl != from && cr != from)) {
             atomicOr(status, GCS_DEV_TREE_MALFORMED);
-            break;
+            have = false;
+            continue;
         }
         int ncl = -1, ncr = -1, nup = -1, nre = 0;
-        if (up >= 0 && up < L.n_internal) {
+        if (up >= 0 && up < ni) {
             ncl = __ldg(&tr[up].child_left);
             ncr = __ldg(&tr[up].child_right);
             nup = __ldg(&bd[up].parent);
@@ -312,31 +343,29 @@ aggregate_kernel(Layout L, const float4* __restrict__ pos,
         // particles of the node and of its two children (the split is the
         // left child's end of the range)
         const int lo_p = min(own, re), hi_p = max(own, re);
-        const int split = cl >= L.n_internal ? cl - L.n_internal : cl + s;
+        const int split = cl >= ni ? cl - ni : cl + s;
         const bool big = fp64 && hi_p - lo_p + 1 >= kComFp64Min;
         const bool big_l = big && split - lo_p + 1 >= kComFp64Min;
         const bool big_r = big && hi_p - split >= kComFp64Min;
         // a local node's internal children are local too: read them from
         // shared memory (their own range end is inside the block)
         ChildData other;
-        if (local && sib < L.n_internal) {
+        if (local && sib < ni) {
             const int so = sib + s - b0;
-            if (so < 0 || so >= kAggThreads) {
+            if (so < 0 || so >= kAggRange) {
                 atomicOr(status, GCS_DEV_TREE_MALFORMED);
-                break;
+                have = false;
+                continue;
             }
             other = from_local(snode[so]);
         } else {
-            other = load_child(sib, L.n_internal, pos, tr, bd, com64, left ? big_r : big_l);
+            other = load_child(sib, ni, pos, tr, bd, com64, left ? big_r : big_l);
         }
         const ChildData& A = left ? mine : other;   // left child
         const ChildData& B = left ? other : mine;   // right child
-        const float3 lo = make_float3(fminf(A.lo.x, B.lo.x), fminf(A.lo.y, B.lo.y),
-                                      fminf(A.lo.z, B.lo.z));
-        const float3 hi = make_float3(fmaxf(A.hi.x, B.hi.x), fmaxf(A.hi.y, B.hi.y),
-                                      fmaxf(A.hi.z, B.hi.z));
-        const float width = fmaxf(__fsub_rn(hi.x, lo.x),
-                                  fmaxf(__fsub_rn(hi.y, lo.y), __fsub_rn(hi.z, lo.z)));
+        const float3 lo = make_float3(fminf(A.lo.x, B.lo.x), fminf(A.lo.y, B.lo.y), fminf(A.lo.z, B.lo.z));
+        const float3 hi = make_float3(fmaxf(A.hi.x, B.hi.x), fmaxf(A.hi.y, B.hi.y), fmaxf(A.hi.z, B.hi.z));
+        const float width = fmaxf(__fsub_rn(hi.x, lo.x), fmaxf(__fsub_rn(hi.y, lo.y), __fsub_rn(hi.z, lo.z)));
         const float m = __fadd_rn(A.m, B.m);
         float3 com;
         ChildData next;
@@ -353,20 +382,18 @@ aggregate_kernel(Layout L, const float4* __restrict__ pos,
                 com = make_float3((float)(next.mx.x / next.md), (float)(next.mx.y / next.md),
                                   (float)(next.mx.z / next.md));
             } else {
-                com = make_float3(com_fp32(A.com.x, A.m, B.com.x, B.m, m),
-                                  com_fp32(A.com.y, A.m, B.com.y, B.m, m),
+                com = make_float3(com_fp32(A.com.x, A.m, B.com.x, B.m, m), com_fp32(A.com.y, A.m, B.com.y, B.m, m),
                                   com_fp32(A.com.z, A.m, B.com.z, B.m, m));
             }
         } else {
-            com = make_float3(__fmul_rn(__fadd_rn(lo.x, hi.x), 0.5f),
-                              __fmul_rn(__fadd_rn(lo.y, hi.y), 0.5f),
+            com = make_float3(__fmul_rn(__fadd_rn(lo.x, hi.x), 0.5f), __fmul_rn(__fadd_rn(lo.y, hi.y), 0.5f),
                               __fmul_rn(__fadd_rn(lo.z, hi.z), 0.5f));
         }
         if (big) com64[node] = make_double4(next.mx.x, next.mx.y, next.mx.z, next.md);
         float4* t4 = reinterpret_cast<float4*>(tr + node);
         t4[0] = make_float4(com.x, com.y, com.z, m);
         tr[node].width = width;
-        if (wnp.wn) write_walk_node(wnp, node, com, m, width, cl, cr, own, re, seg_lo, seg_hi, L.n_internal);
+        if (wnp.wn) write_walk_node(wnp, node, com, m, width, cl, cr, own, re, seg_lo, seg_hi, ni);
         float4* b4 = reinterpret_cast<float4*>(bd + node);
         b4[0] = make_float4(lo.x, lo.y, lo.z, hi.x);
         reinterpret_cast<float2*>(b4 + 1)[0] = make_float2(hi.y, hi.z);
@@ -388,6 +415,7 @@ aggregate_kernel(Layout L, const float4* __restrict__ pos,
         cr = ncr;
         up = nup;
         re = nre;
+        have = node >= 0;  // the root ends the climb
     }
 }
 
@@ -408,7 +436,8 @@ void launch_aggregate(const Layout& L, const float4* pos, BvhNodeTraverse* tr, B
                       double4* com64, const int32_t* leaf_parent, int com_fp64, const WalkNodeParams& wnp,
                       uint32_t* status, cudaStream_t st) {
     if (L.n <= 0) return;
-    aggregate_kernel<<<tree_grid(L.n), kAggThreads, 0, st>>>(L, pos, tr, bd, com64, leaf_parent, com_fp64,
+    const unsigned blocks = (unsigned)((L.n + kAggRange - 1) / kAggRange);
+    aggregate_kernel<<<blocks, kAggThreads, 0, st>>>(L, pos, tr, bd, com64, leaf_parent, com_fp64,
                                                              wnp, status);
 }
 
