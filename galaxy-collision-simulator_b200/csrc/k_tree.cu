@@ -12,8 +12,9 @@
 // builds for that segment alone.  Each node also records the far end of its
 // particle range, which gives the walk the node's particle count.
 //
-// Aggregation: one thread per particle climbs from its leaf; at each node the
-// first arrival stops and the second computes the node from both children
+// Aggregation: a climb starts at every particle's leaf (a lane runs one climb
+// after another over its block's particles); at each node the first arrival
+// stops and the second computes the node from both children
 // (karras_bvh.cuh:175-225).  Unlike the reference, the arrival counter is a
 // release/acquire handshake (__threadfence on both sides and L2-coherent
 // loads of the children), so the second arrival always sees the first one's
