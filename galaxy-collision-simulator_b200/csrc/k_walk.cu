@@ -981,7 +981,7 @@ partition_kernel(const float4* __restrict__ pos, const SuperGroup* __restrict__ 
 // scans; a list or stack that would overflow, or more pops than the segment
 // has internal nodes, marks the super-group invalid (its groups then walk
 // from the root), so nothing is written out of bounds.
-constexpr int kFrontWarps = 8;
+constexpr int kFrontWarps = 4;  // 1,024 blocks for 4,096 super-groups: better spread over the SMs than 8
 constexpr int kFrontStack = 1024;
 constexpr int kFrontSlots = 2;  // nodes per lane per round
 
