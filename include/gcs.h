@@ -166,9 +166,11 @@ int gcs_step(gcs_ctx* ctx, const gcs_params* p);
  * arrays) and recaptures only when the parameters, the segment layout, the
  * group width or the stream change.  Needs a non-default stream. */
 int gcs_set_graphs(gcs_ctx* ctx, int32_t enable);
-/* Timing hooks: `start` and `end` (cudaEvent_t, or NULL) are recorded on the
- * context stream right before and after every walk stage from now on, in
- * eager steps and inside graph-captured steps alike (there they are
+/* Timing hooks: `start` and `end` (cudaEvent_t of the context's device, or
+ * NULL) are recorded on the context stream right before and after the walk
+ * stage of every gcs_step and gcs_run_stages from now on (not in the host
+ * steps, gcs_step_host and gcs_step_host_io), in eager steps and inside
+ * graph-captured steps alike (there they are
  * event-record nodes; a gcs_step after a change of events points those nodes
  * at the new events before it launches, so each step can be timed with its
  * own pair).  Setting or clearing an event recaptures the graphs at the next
