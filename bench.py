@@ -11,11 +11,13 @@ path shards by scenario with no data-path collective, so scaling is weak.
 
 value   = N_particles * K * ranks / (max over ranks of the device time of K
           steps), inputs resident in HBM (the 1M-particle working set,
-          ~270 MB, is larger than the 126 MB L2; no flush needed);
+          ~270 MB, is larger than the 126 MB L2; no flush needed); each step
+          is one launch of the library's captured CUDA graph of the step;
 e2e     = the same metric through the C ABI with host buffers: every step
           copies the Star array in from pinned host memory and the stepped
-          Star array back out (gcs_upload_stars + gcs_step_host);
-roofline= the walk kernel (the dominant stage) against the FP32 FMA-pipe
+          Star array back out (gcs_step_host_io);
+roofline= the walk stage (the dominant one, timed by events the library
+          records around it inside the graph) against the FP32 FMA-pipe
           peak: 20 flops per interaction (monopole or particle term),
           interactions counted by the counting walk on the same state;
 cpu_baseline = the reference's own CPU Barnes-Hut (oracle/_ref/libref_cpu.so:
